@@ -1,0 +1,154 @@
+/*
+ * vie_b200.h -- C ABI of the B200 VIE-FFT library (libvie_b200.so).
+ *
+ * Plain pointers and sizes only.  Host arrays follow the reference layout:
+ * C order (last index fastest) over (nx, ny, nz) like Memory3D buffers
+ * (common.h:68-94); complex values are interleaved (re, im) doubles like
+ * MKL_Complex16; a vector of the three current / field components is one
+ * block of 3*a complex values (x, then y, then z), a = nx*ny*nz.
+ * Permittivities use the reference's exp(+j omega t) sign convention: lossy
+ * media have a NEGATIVE imaginary part (data/Au_epr.txt).
+ *
+ * Every function returns a status code (VIE_OK = 0) and leaves a message for
+ * vie_last_error().  The reference checks no status at all; the drop-in
+ * headers (dropin/*.h) turn a non-zero status into a message on stderr and
+ * exit(1).
+ *
+ * One context = one grid on one GPU with one CUDA stream.  Contexts are
+ * independent; a single context is not safe for concurrent calls.
+ */
+#ifndef VIE_B200_H
+#define VIE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define VIE_API __attribute__((visibility("default")))
+#else
+#define VIE_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define VIE_OK 0
+#define VIE_ERR_ARG 1        /* bad argument or size */
+#define VIE_ERR_ALLOC 2      /* device or host allocation failed */
+#define VIE_ERR_CUDA 3       /* CUDA runtime error */
+#define VIE_ERR_BREAKDOWN 4  /* Krylov breakdown (zero denominator) */
+#define VIE_ERR_MAXIT 5      /* iteration cap reached before the tolerance */
+#define VIE_ERR_NAN 6        /* NaN / Inf in the iteration */
+#define VIE_ERR_STATE 7      /* call order (e.g. solve before vie_green) */
+#define VIE_ERR_TIMEOUT 8    /* a bounded device wait expired */
+#define VIE_ERR_NODEVICE 9   /* no CUDA device */
+
+/* solvers: the reference's Iteration_Type values (CG_Iteration.h:47) */
+#define VIE_SOLVER_CG 1         /* CGNR, CG_FFT (CG_Iteration.h:176-357) */
+#define VIE_SOLVER_BICG 2       /* complex-symmetric BiCG, BICG_FFT (:360-528) */
+#define VIE_SOLVER_BICGSTAB 3   /* BICGSTAB_FFT (:531-776), the reference default */
+#define VIE_SOLVER_CORS 4       /* CORS_FFT (:780-1073) */
+#define VIE_SOLVER_BICORSTAB 5  /* BICORSTAB_FFT (:1076-1362) */
+
+/* arithmetic of a solve */
+#define VIE_PREC_FP64 0   /* every operation in FP64 complex */
+#define VIE_PREC_MIXED 1  /* FP32-complex inner Krylov inside FP64 defect correction */
+
+typedef struct vie_ctx vie_ctx;
+
+typedef struct {
+    int nx, ny, nz;      /* grid, Nx/Ny/Nz of Model.h:32-34 (each >= 2) */
+    double dx, dy, dz;   /* cell sizes delta_x/y/z (Model.h:28-30), in the reference's 100 nm unit */
+    double k0;           /* free-space wavenumber (Model.h:25) */
+    int device;          /* CUDA device ordinal */
+} vie_grid;
+
+/* Create a context for one grid.  Replaces the allocation part of
+   Parameter_Input (Model.h:172-201) for the arrays the hot path owns. */
+VIE_API int vie_create(const vie_grid* g, vie_ctx** out);
+VIE_API void vie_destroy(vie_ctx* ctx);
+VIE_API const char* vie_last_error(const vie_ctx* ctx);
+VIE_API const char* vie_status_string(int status);
+
+/* Geometry.  material: a bytes of indices into a permittivity table of
+   n_materials entries (the reference's Material with Real_EPR / Imag_EPR,
+   Model.h:17, 81-83; index 0 is the air dummy 1.1).  Equivalent per-voxel
+   form: vie_set_eps with a complex values. */
+VIE_API int vie_set_material(vie_ctx* ctx, const uint8_t* material, const double* eps_re, const double* eps_im,
+                     int n_materials);
+VIE_API int vie_set_eps(vie_ctx* ctx, const double* eps);
+/* Edge flags Flag_X, Flag_Y, Flag_Z (Model.h:21-23, GetFlag Model.h:335-398), a bytes each. */
+VIE_API int vie_set_flags(vie_ctx* ctx, const uint8_t* fx, const uint8_t* fy, const uint8_t* fz);
+
+/* Green_Function_Compute (GreenFunction.h:8-141), on the GPU in FP64.  The
+   spectrum is kept as its (nx+1)(ny+1)(nz+1) even-symmetric octant. */
+VIE_API int vie_green(vie_ctx* ctx);
+/* The natural-order (2nx, 2ny, 2nz) spectrum the reference stores in
+   Green_Function after Green_Function_Compute. out: 8a complex. */
+VIE_API int vie_green_spectrum(vie_ctx* ctx, double* out);
+
+/* Incident_Wave (GreenFunction.h:144-248), on the GPU in FP64.  The field
+   becomes the right-hand side of the next solve; out (3a complex) may be NULL. */
+VIE_API int vie_incident(vie_ctx* ctx, double theta, double phi, double psi, double* out);
+/* Right-hand side from the host (Ex_inc, Ey_inc, Ez_inc; 3a complex). */
+VIE_API int vie_set_rhs(vie_ctx* ctx, const double* e);
+
+/* One operator application y = A x, or y = A^H x when conj != 0, with host
+   buffers (3a complex each), exactly as the drivers compose it: zeroed field,
+   X_FFT/Y_FFT/Z_FFT (CG_Iteration.h:131-173) or the _Conjugate twins
+   (:86-128), then Current_Reset (fft.h:13-35). */
+VIE_API int vie_matvec(vie_ctx* ctx, const double* x, double* y, int conj);
+/* Same on device buffers of the context's GPU.  precision VIE_PREC_FP64:
+   x, y are 3a double2; VIE_PREC_MIXED: 3a float2 (the FP32 operator).
+   Runs on the context stream; returns after the launch (no sync). */
+VIE_API int vie_matvec_dev(vie_ctx* ctx, const void* x, void* y, int conj, int precision);
+
+typedef struct {
+    int solver;         /* VIE_SOLVER_* */
+    int precision;      /* VIE_PREC_FP64 or VIE_PREC_MIXED */
+    double tol;         /* relative-residual threshold (CG_THR, CG_Iteration.h:46) */
+    int max_iter;       /* iteration cap; <= 0 means nx*ny*nz like the reference */
+    double inner_tol;   /* mixed: inner reduction per refinement step (<= 0: 1e-4) */
+    int max_outer;      /* mixed: refinement cap (<= 0: 30) */
+    int verbose;        /* print "CG Error" per iteration like the reference */
+} vie_solve_params;
+
+typedef struct {
+    int steps;          /* index m of the converged iteration ("Steps: m"), as the reference prints */
+    int iterations;     /* Krylov iterations executed (sum of inner ones when mixed) */
+    int outer;          /* refinement steps (mixed) */
+    int matvecs_fp64;   /* operator applications in FP64 */
+    int matvecs_fp32;   /* operator applications in FP32 */
+    double relres;      /* the solver's own residual estimate at exit */
+    double true_relres; /* ||b - A x|| / ||b|| evaluated in FP64 at exit */
+    double seconds;     /* device time of the solve */
+} vie_solve_info;
+
+/* Solve A x = b for the current right-hand side from x0 = 0.  Replaces
+   FFT_Program (CG_Iteration.h:1365-1388) and the driver it dispatches to.
+   x (3a complex) may be NULL; the solution also stays on the device. */
+VIE_API int vie_solve(vie_ctx* ctx, const vie_solve_params* p, double* x, vie_solve_info* info);
+/* Copy the last solution (Current_X/Y/Z) to the host, 3a complex. */
+VIE_API int vie_get_solution(vie_ctx* ctx, double* x);
+/* Device pointer of the last solution (3a double2), valid until the next solve. */
+VIE_API int vie_solution_device(vie_ctx* ctx, const void** x);
+
+/* Device pointers and byte sizes of the context's FP64 right-hand side and
+   solution, for callers that keep data on the GPU. */
+VIE_API int vie_rhs_device(vie_ctx* ctx, void** rhs);
+
+/* Synchronise the context stream. */
+VIE_API int vie_sync(vie_ctx* ctx);
+/* The context's CUDA stream (a cudaStream_t), for callers that order their
+   own work or record timing events on it. */
+VIE_API int vie_stream(vie_ctx* ctx, void** stream);
+
+/* Library version string. */
+VIE_API const char* vie_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

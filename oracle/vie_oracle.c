@@ -11,6 +11,7 @@
 #include "vie_oracle.h"
 #include "vo_fft.h"
 
+#include <complex.h>
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
@@ -29,14 +30,10 @@ static inline cx mul(cx a, cx b) { return mk(a.re * b.re - a.im * b.im, a.re * b
 static inline cx scl(cx a, double s) { return mk(a.re * s, a.im * s); }
 static inline cx cj(cx a) { return mk(a.re, -a.im); }
 static inline cx cdiv(cx a, cx b) {
-    /* scaled division (Smith), well conditioned for the magnitudes here */
-    if (fabs(b.re) >= fabs(b.im)) {
-        double r = b.im / b.re, d = b.re + b.im * r;
-        return mk((a.re + a.im * r) / d, (a.im - a.re * r) / d);
-    } else {
-        double r = b.re / b.im, d = b.re * r + b.im;
-        return mk((a.re * r + a.im) / d, (a.im * r - a.re) / d);
-    }
+    /* C99 complex division: the same library routine as std::complex<double>
+       operator/ in the reference, so the quotients agree bit for bit */
+    double complex r = CMPLX(a.re, a.im) / CMPLX(b.re, b.im);
+    return mk(creal(r), cimag(r));
 }
 static inline cx cexpi(double t) { return mk(cos(t), sin(t)); } /* exp(i t) */
 
@@ -93,12 +90,19 @@ int vo_green(const vo_grid* g, double* out) {
 /* ------------------------------------------------------------------------ */
 /* Incident_Wave, GreenFunction.h:144-248                                   */
 /* ------------------------------------------------------------------------ */
-/* edge integral of exp(-i k s) over a cell of length d, times the point phase */
+/* edge integral of exp(-i k s) over a cell of length d, times the point phase,
+   in the reference's complex arithmetic (GreenFunction.h:182-194) */
 static cx edge_phase(double phase, double kk, double d) {
-    cx e = cexpi(-phase);
-    if (fabs(kk) < EPSC) return scl(e, d);               /* :187-190 */
-    /* (exp(-i k d/2) - exp(i k d/2)) / (-i k) = 2 sin(k d / 2) / k   (:193) */
-    return scl(e, 2.0 * sin(kk * d / 2.0) / kk);
+    double complex V1 = CMPLX(0.0, -phase);
+    double complex V4;
+    if (fabs(kk) < EPSC) {
+        V4 = cexp(V1) * d;                                  /* :187-190 */
+    } else {
+        double complex V2 = CMPLX(0.0, -(kk * d / 2.0));
+        double complex V3 = CMPLX(0.0, (kk * d / 2.0));
+        V4 = cexp(V1) * (cexp(V2) - cexp(V3)) / CMPLX(0.0, -kk);   /* :193 */
+    }
+    return mk(creal(V4), cimag(V4));
 }
 
 int vo_incident(const vo_grid* g, double theta, double phi, double psi, double* e) {
@@ -110,7 +114,6 @@ int vo_incident(const vo_grid* g, double theta, double phi, double psi, double* 
     const double kz = g->k0 * cos(th);
     const double px = cos(th) * cos(ph) * cos(ps) - sin(ph) * sin(ps);  /* :196-199 */
     const double py = cos(th) * sin(ph) * cos(ps) + cos(ph) * sin(ps);  /* :219-222 */
-    const double pz = -sin(th) * cos(ps);                               /* :243-244 */
     cx* ex = (cx*)e;
     cx* ey = ex + a;
     cx* ez = ey + a;
@@ -124,7 +127,9 @@ int vo_incident(const vo_grid* g, double theta, double phi, double psi, double* 
                 xm = (i + 0.5) * g->dx; ym = (j + 1) * g->dy; zm = (k + 0.5) * g->dz;
                 ey[v] = scl(edge_phase(kx * xm + ky * ym + kz * zm, ky, g->dy), py);
                 xm = (i + 0.5) * g->dx; ym = (j + 0.5) * g->dy; zm = (k + 1) * g->dz;
-                ez[v] = scl(edge_phase(kx * xm + ky * ym + kz * zm, kz, g->dz), pz);
+                /* -real(V4)*sin(theta)*cos(psi), evaluated left to right as :243-244 */
+                cx vz = edge_phase(kx * xm + ky * ym + kz * zm, kz, g->dz);
+                ez[v] = mk(-vz.re * sin(th) * cos(ps), -vz.im * sin(th) * cos(ps));
             }
     return 0;
 }

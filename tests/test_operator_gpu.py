@@ -1,0 +1,134 @@
+"""CUDA operator parity: Green spectrum, incident field, A x and A^H x in FP64
+and FP32 against the reference's outputs (golden fixtures from oracle/_ref)
+and the oracle restatement, plus size-independent properties at full sizes."""
+import os
+
+import numpy as np
+import pytest
+
+import vie_fft_b200 as V
+from oracle import oracle as O
+from tests.golden import make_golden as MG
+from vie_fft_b200 import geometry as GEO
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+# tolerances: FP64 results are compared relative to the largest magnitude
+FP64_TOL = 1e-12
+FP32_TOL = 2e-5
+
+
+def rel(a, b):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def make_ctx(shape, d, k0, material, flags, table=None, eps=None):
+    c = V.Context(*shape, *d, k0)
+    c.set_flags(flags)
+    if eps is not None:
+        c.set_eps(eps)
+    else:
+        c.set_material(material, table)
+    c.green()
+    return c
+
+
+@pytest.mark.parametrize("idx", range(len(MG.SMALL)))
+def test_small_cases_match_reference(idx):
+    gold = np.load(os.path.join(GOLD, "small_ops.npz"))
+    shape, d, k0, ang, mat, flags, x = MG.small_inputs(idx)
+    with make_ctx(shape, d, k0, mat, flags, MG.EPS_TABLE) as c:
+        assert rel(c.green_spectrum(), gold[f"green{idx}"]) < 1e-13
+        assert rel(c.incident(*ang), gold[f"inc{idx}"]) < 1e-13
+        assert rel(c.matvec(x, conj=False), gold[f"ax{idx}"]) < FP64_TOL
+        assert rel(c.matvec(x, conj=True), gold[f"ahx{idx}"]) < FP64_TOL
+
+
+@pytest.mark.parametrize("shape", [(24, 20, 16), (31, 17, 13), (48, 40, 56), (9, 7, 5), (2, 2, 2), (16, 3, 64)])
+def test_matvec_fp64_matches_oracle(shape):
+    rng = np.random.default_rng(sum(shape))
+    d = (0.01, 0.012, 0.011)
+    k0 = GEO.k0_of(530.0)
+    table = np.array([1.1, 2.4 - 0.05j, -8.5 - 0.3j, 3.8 - 0.6j])
+    mat = rng.integers(0, 4, size=shape).astype(np.uint8)
+    flags = rng.integers(0, 2, size=(3,) + shape).astype(np.uint8)
+    x = rng.standard_normal((3,) + shape) + 1j * rng.standard_normal((3,) + shape)
+    g = O.Grid(*shape, *d, k0)
+    G = O.green(g)
+    with make_ctx(shape, d, k0, mat, flags, table) as c:
+        for conj in (False, True):
+            assert rel(c.matvec(x, conj), O.matvec(g, G, table[mat], flags, x, conj)) < FP64_TOL
+
+
+def _torch():
+    torch = pytest.importorskip("torch")
+    assert torch.cuda.is_available(), "GPU tests need CUDA"
+    return torch
+
+
+@pytest.mark.parametrize("shape", [(24, 20, 16), (31, 17, 13)])
+def test_matvec_fp32_matches_oracle(shape):
+    torch = _torch()
+    rng = np.random.default_rng(5)
+    d = (0.01, 0.01, 0.01)
+    k0 = GEO.k0_of(450.0)
+    table = np.array([1.1, 2.4 - 0.05j, -4.4 - 0.2j, 3.8 - 0.6j])
+    mat = rng.integers(0, 4, size=shape).astype(np.uint8)
+    flags = rng.integers(0, 2, size=(3,) + shape).astype(np.uint8)
+    x = rng.standard_normal((3,) + shape) + 1j * rng.standard_normal((3,) + shape)
+    g = O.Grid(*shape, *d, k0)
+    ref = O.matvec(g, O.green(g), table[mat], flags, x, False)
+    with make_ctx(shape, d, k0, mat, flags, table) as c:
+        xt = torch.from_numpy(x.astype(np.complex64)).cuda()
+        yt = torch.zeros_like(xt)
+        torch.cuda.synchronize()
+        c.matvec_dev(xt.data_ptr(), yt.data_ptr(), conj=False, precision=V.PREC_MIXED)
+        c.sync()
+        assert rel(yt.cpu().numpy(), ref) < FP32_TOL
+
+
+def test_adjoint_and_symmetry_identities_full_size():
+    """<y, A x> = <A^H y, x> and, for cubic voxels on flagged edges, y^T A x = x^T A y."""
+    w = GEO.solar_cell(shape=(96, 96, 48), nspheres=4, radius_nm=8.0, spacer_nm=8.0, active_nm=24.0,
+                       sphere_z_nm=(16.0, 24.0))
+    rng = np.random.default_rng(11)
+    mask = w.flags.astype(bool)
+    x = (rng.standard_normal((3,) + w.shape) + 1j * rng.standard_normal((3,) + w.shape)) * mask
+    y = (rng.standard_normal((3,) + w.shape) + 1j * rng.standard_normal((3,) + w.shape)) * mask
+    with make_ctx(w.shape, w.d, w.k0, w.material, w.flags, w.eps_table) as c:
+        Ax, Ay, AHy = c.matvec(x), c.matvec(y), c.matvec(y, conj=True)
+    lhs = np.vdot(y, Ax)
+    assert abs(lhs - np.vdot(AHy, x)) < 1e-12 * np.linalg.norm(y) * np.linalg.norm(Ax)
+    assert abs(np.sum(y * Ax) - np.sum(x * Ay)) < 1e-12 * np.linalg.norm(y) * np.linalg.norm(Ax)
+
+
+def test_linearity_and_fp32_consistency_128():
+    torch = _torch()
+    w = GEO.sphere_cluster(n=128, count=40, seed=2)
+    rng = np.random.default_rng(12)
+    x = rng.standard_normal((3,) + w.shape) + 1j * rng.standard_normal((3,) + w.shape)
+    y = rng.standard_normal((3,) + w.shape) + 1j * rng.standard_normal((3,) + w.shape)
+    with make_ctx(w.shape, w.d, w.k0, w.material, w.flags, w.eps_table) as c:
+        Ax, Ay = c.matvec(x), c.matvec(y)
+        al, be = 0.3 - 1.2j, -0.7 + 0.4j
+        assert rel(c.matvec(al * x + be * y), al * Ax + be * Ay) < 1e-12
+        xt = torch.from_numpy(x.astype(np.complex64)).cuda()
+        yt = torch.zeros_like(xt)
+        torch.cuda.synchronize()
+        c.matvec_dev(xt.data_ptr(), yt.data_ptr(), precision=V.PREC_MIXED)
+        c.sync()
+        assert rel(yt.cpu().numpy(), Ax) < FP32_TOL
+
+
+def test_operator_state_errors():
+    with V.Context(8, 8, 8, 0.01, 0.01, 0.01, 1.0) as c:
+        with pytest.raises(V.VieError) as e:
+            c.matvec(np.zeros((3, 8, 8, 8)))
+        assert e.value.status == V.VIE_ERR_STATE
+        with pytest.raises(V.VieError) as e:
+            c.set_material(np.full((8, 8, 8), 5, np.uint8), [1.1, 2.0])
+        assert e.value.status == V.VIE_ERR_ARG
+        with pytest.raises(V.VieError) as e:
+            c.set_eps(np.ones((8, 8, 8), complex))  # eps = 1 has no inverse contrast
+        assert e.value.status == V.VIE_ERR_ARG

@@ -1,0 +1,336 @@
+// vie_capi.cu -- the extern "C" entry points declared in include/vie_b200.h.
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+
+#include "vie_internal.h"
+
+namespace vie {
+int green_compute(vie_ctx* ctx);
+int green_expand(vie_ctx* ctx, double2* d_out);
+int incident_compute(vie_ctx* ctx, double theta, double phi, double psi, double2* d_e);
+int solve_driver(vie_ctx* ctx, const vie_solve_params* prm, vie_solve_info* info);
+}  // namespace vie
+
+using namespace vie;
+
+namespace {
+
+int check_ctx(vie_ctx* ctx) { return ctx ? VIE_OK : VIE_ERR_ARG; }
+
+#define CTX_CUDA(expr)                                                                     \
+    do {                                                                                   \
+        cudaError_t e__ = (expr);                                                          \
+        if (e__ != cudaSuccess) return ctx->set_error(VIE_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e__)); \
+    } while (0)
+
+// (Re)build both operators once flags exist (tables do not depend on eps or Green).
+// Tile sizes: defaults chosen per precision by Operator::init; the
+// environment variable VIE_TILES="tz,tc,tx" overrides them (tuning runs).
+TileCfg tiles_from_env() {
+    TileCfg t{};
+    if (const char* s = std::getenv("VIE_TILES")) {
+        int a = 0, b = 0, c = 0;
+        if (std::sscanf(s, "%d,%d,%d", &a, &b, &c) == 3) { t.tz = a; t.tc = b; t.tx = c; }
+    }
+    return t;
+}
+
+int ensure_operators(vie_ctx* ctx) {
+    if (ctx->op64.ready && ctx->op32.ready) return VIE_OK;
+    TileCfg t = tiles_from_env();
+    int rc = ctx->op64.init(ctx->nx, ctx->ny, ctx->nz, ctx->d, ctx->k0, t, ctx->plans, ctx->d_flags, ctx->err);
+    if (rc) return rc;
+    rc = ctx->op32.init(ctx->nx, ctx->ny, ctx->nz, ctx->d, ctx->k0, t, ctx->plans, ctx->d_flags, ctx->err);
+    return rc;
+}
+
+int ready_for_operator(vie_ctx* ctx) {
+    if (!ctx->have_flags) return ctx->set_error(VIE_ERR_STATE, "edge flags not set (vie_set_flags)");
+    if (!ctx->have_eps) return ctx->set_error(VIE_ERR_STATE, "permittivity not set (vie_set_material / vie_set_eps)");
+    if (!ctx->have_green) return ctx->set_error(VIE_ERR_STATE, "Green's function not computed (vie_green)");
+    return VIE_OK;
+}
+
+int upload_contrast(vie_ctx* ctx) {
+    int rc = ensure_operators(ctx);
+    if (rc) return rc;
+    rc = ctx->op64.set_contrast(ctx->w_host.data(), ctx->stream, ctx->err);
+    if (rc) return rc;
+    return ctx->op32.set_contrast(ctx->w_host.data(), ctx->stream, ctx->err);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* vie_version(void) { return "vie_b200 0.1 (sm_100a)"; }
+
+const char* vie_status_string(int s) {
+    switch (s) {
+        case VIE_OK: return "ok";
+        case VIE_ERR_ARG: return "invalid argument";
+        case VIE_ERR_ALLOC: return "allocation failed";
+        case VIE_ERR_CUDA: return "CUDA error";
+        case VIE_ERR_BREAKDOWN: return "Krylov breakdown";
+        case VIE_ERR_MAXIT: return "iteration cap reached";
+        case VIE_ERR_NAN: return "non-finite value";
+        case VIE_ERR_STATE: return "call order";
+        case VIE_ERR_TIMEOUT: return "device wait timed out";
+        case VIE_ERR_NODEVICE: return "no CUDA device";
+        default: return "unknown status";
+    }
+}
+
+const char* vie_last_error(const vie_ctx* ctx) { return ctx ? ctx->err.msg.c_str() : "null context"; }
+
+int vie_create(const vie_grid* g, vie_ctx** out) {
+    if (!g || !out) return VIE_ERR_ARG;
+    *out = nullptr;
+    if (g->nx < 2 || g->ny < 2 || g->nz < 2 || !(g->dx > 0) || !(g->dy > 0) || !(g->dz > 0) || !(g->k0 > 0))
+        return VIE_ERR_ARG;
+    if (g->nx > 65535 || g->ny > 32767 || g->nz > 65535) return VIE_ERR_ARG;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return VIE_ERR_NODEVICE;
+    if (g->device < 0 || g->device >= ndev) return VIE_ERR_ARG;
+    vie_ctx* ctx = new (std::nothrow) vie_ctx();
+    if (!ctx) return VIE_ERR_ALLOC;
+    ctx->device = g->device;
+    ctx->nx = g->nx; ctx->ny = g->ny; ctx->nz = g->nz;
+    ctx->a = (long long)g->nx * g->ny * g->nz;
+    ctx->d[0] = g->dx; ctx->d[1] = g->dy; ctx->d[2] = g->dz;
+    ctx->k0 = g->k0;
+    const int n3[3] = {g->nx, g->ny, g->nz};
+    for (int ax = 0; ax < 3; ax++) ctx->plans[ax] = make_axis_plan(n3[ax]);
+    if (cudaSetDevice(g->device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMalloc(&ctx->d_flags, (size_t)ctx->a) != cudaSuccess ||
+        cudaMalloc(&ctx->d_rhs, sizeof(double2) * 3 * (size_t)ctx->a) != cudaSuccess ||
+        cudaMalloc(&ctx->d_x, sizeof(double2) * 3 * (size_t)ctx->a) != cudaSuccess) {
+        vie_destroy(ctx);
+        return VIE_ERR_ALLOC;
+    }
+    cudaMemset(ctx->d_flags, 0, (size_t)ctx->a);
+    cudaMemset(ctx->d_x, 0, sizeof(double2) * 3 * (size_t)ctx->a);
+    ctx->w_host.assign(2 * (size_t)ctx->a, 0.0);
+    *out = ctx;
+    return VIE_OK;
+}
+
+void vie_destroy(vie_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    ctx->op64.release();
+    ctx->op32.release();
+    if (ctx->d_flags) cudaFree(ctx->d_flags);
+    if (ctx->d_green) cudaFree(ctx->d_green);
+    if (ctx->d_rhs) cudaFree(ctx->d_rhs);
+    if (ctx->d_x) cudaFree(ctx->d_x);
+    for (size_t i = 0; i < ctx->work.size(); i += 2)
+        if (ctx->work[i]) cudaFree(ctx->work[i]);
+    if (ctx->d_scal) cudaFree(ctx->d_scal);
+    if (ctx->d_partial) cudaFree(ctx->d_partial);
+    if (ctx->h_scal) cudaFreeHost(ctx->h_scal);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+int vie_set_eps(vie_ctx* ctx, const double* eps) {
+    if (check_ctx(ctx) || !eps) return VIE_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    // w = 1/(eps - 1), the per-voxel factor of the diagonal term (fft.h:430-432)
+    for (long long v = 0; v < ctx->a; v++) {
+        const std::complex<double> e(eps[2 * v] - 1.0, eps[2 * v + 1]);
+        if (e == std::complex<double>(0.0, 0.0))
+            return ctx->set_error(VIE_ERR_ARG, "permittivity equal to 1 (zero contrast) at voxel " + std::to_string(v));
+        const std::complex<double> w = 1.0 / e;
+        ctx->w_host[2 * v] = w.real();
+        ctx->w_host[2 * v + 1] = w.imag();
+    }
+    ctx->have_eps = true;
+    if (!ctx->have_flags) return VIE_OK;
+    return upload_contrast(ctx);
+}
+
+int vie_set_material(vie_ctx* ctx, const uint8_t* material, const double* eps_re, const double* eps_im,
+                     int n_materials) {
+    if (check_ctx(ctx) || !material || !eps_re || !eps_im || n_materials < 1 || n_materials > 256)
+        return VIE_ERR_ARG;
+    std::vector<double> eps(2 * (size_t)ctx->a);
+    for (long long v = 0; v < ctx->a; v++) {
+        const int m = material[v];
+        if (m >= n_materials) return ctx->set_error(VIE_ERR_ARG, "material index outside the permittivity table");
+        eps[2 * v] = eps_re[m];
+        eps[2 * v + 1] = eps_im[m];
+    }
+    return vie_set_eps(ctx, eps.data());
+}
+
+int vie_set_flags(vie_ctx* ctx, const uint8_t* fx, const uint8_t* fy, const uint8_t* fz) {
+    if (check_ctx(ctx) || !fx || !fy || !fz) return VIE_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    std::vector<uint8_t> packed((size_t)ctx->a);
+    for (long long v = 0; v < ctx->a; v++)
+        packed[v] = (uint8_t)((fx[v] ? 1 : 0) | (fy[v] ? 2 : 0) | (fz[v] ? 4 : 0));
+    CTX_CUDA(cudaMemcpy(ctx->d_flags, packed.data(), (size_t)ctx->a, cudaMemcpyHostToDevice));
+    ctx->have_flags = true;
+    int rc = ensure_operators(ctx);
+    if (rc) return rc;
+    if (ctx->have_eps) rc = upload_contrast(ctx);
+    if (!rc && ctx->have_green) {
+        rc = ctx->op64.set_green(ctx->d_green, ctx->k0, ctx->stream, ctx->err);
+        if (!rc) rc = ctx->op32.set_green(ctx->d_green, ctx->k0, ctx->stream, ctx->err);
+    }
+    return rc;
+}
+
+int vie_green(vie_ctx* ctx) {
+    if (check_ctx(ctx)) return VIE_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    int rc = green_compute(ctx);
+    if (rc) return rc;
+    ctx->have_green = true;
+    if (ctx->op64.ready) {
+        rc = ctx->op64.set_green(ctx->d_green, ctx->k0, ctx->stream, ctx->err);
+        if (!rc) rc = ctx->op32.set_green(ctx->d_green, ctx->k0, ctx->stream, ctx->err);
+        if (rc) return rc;
+    }
+    CTX_CUDA(cudaStreamSynchronize(ctx->stream));
+    return VIE_OK;
+}
+
+int vie_green_spectrum(vie_ctx* ctx, double* out) {
+    if (check_ctx(ctx) || !out) return VIE_ERR_ARG;
+    if (!ctx->have_green) return ctx->set_error(VIE_ERR_STATE, "Green's function not computed (vie_green)");
+    cudaSetDevice(ctx->device);
+    const size_t m = 8 * (size_t)ctx->a;
+    double2* d = nullptr;
+    CTX_CUDA(cudaMalloc(&d, sizeof(double2) * m));
+    int rc = green_expand(ctx, d);
+    if (!rc) {
+        cudaError_t e = cudaMemcpyAsync(out, d, sizeof(double2) * m, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) rc = ctx->set_error(VIE_ERR_CUDA, cudaGetErrorString(e));
+    }
+    cudaFree(d);
+    return rc;
+}
+
+int vie_incident(vie_ctx* ctx, double theta, double phi, double psi, double* out) {
+    if (check_ctx(ctx)) return VIE_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    int rc = incident_compute(ctx, theta, phi, psi, ctx->d_rhs);
+    if (rc) return rc;
+    ctx->have_rhs = true;
+    if (out) {
+        CTX_CUDA(cudaMemcpyAsync(out, ctx->d_rhs, sizeof(double2) * 3 * (size_t)ctx->a, cudaMemcpyDeviceToHost,
+                                 ctx->stream));
+    }
+    CTX_CUDA(cudaStreamSynchronize(ctx->stream));
+    return VIE_OK;
+}
+
+int vie_set_rhs(vie_ctx* ctx, const double* e) {
+    if (check_ctx(ctx) || !e) return VIE_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    CTX_CUDA(cudaMemcpyAsync(ctx->d_rhs, e, sizeof(double2) * 3 * (size_t)ctx->a, cudaMemcpyHostToDevice, ctx->stream));
+    CTX_CUDA(cudaStreamSynchronize(ctx->stream));
+    ctx->have_rhs = true;
+    return VIE_OK;
+}
+
+int vie_rhs_device(vie_ctx* ctx, void** rhs) {
+    if (check_ctx(ctx) || !rhs) return VIE_ERR_ARG;
+    *rhs = ctx->d_rhs;
+    ctx->have_rhs = true;
+    return VIE_OK;
+}
+
+int vie_matvec_dev(vie_ctx* ctx, const void* x, void* y, int conj, int precision) {
+    if (check_ctx(ctx) || !x || !y) return VIE_ERR_ARG;
+    int rc = ready_for_operator(ctx);
+    if (rc) return rc;
+    cudaSetDevice(ctx->device);
+    if (precision == VIE_PREC_FP64)
+        return ctx->op64.apply((const double2*)x, (double2*)y, conj != 0, ctx->stream, ctx->err);
+    if (precision == VIE_PREC_MIXED)
+        return ctx->op32.apply((const float2*)x, (float2*)y, conj != 0, ctx->stream, ctx->err);
+    return ctx->set_error(VIE_ERR_ARG, "precision must be VIE_PREC_FP64 or VIE_PREC_MIXED");
+}
+
+int vie_matvec(vie_ctx* ctx, const double* x, double* y, int conj) {
+    if (check_ctx(ctx) || !x || !y) return VIE_ERR_ARG;
+    int rc = ready_for_operator(ctx);
+    if (rc) return rc;
+    cudaSetDevice(ctx->device);
+    const size_t bytes = sizeof(double2) * 3 * (size_t)ctx->a;
+    double2 *dx = nullptr, *dy = nullptr;
+    CTX_CUDA(cudaMalloc(&dx, bytes));
+    if (cudaMalloc(&dy, bytes) != cudaSuccess) {
+        cudaFree(dx);
+        return ctx->set_error(VIE_ERR_ALLOC, "device allocation failed");
+    }
+    cudaError_t e = cudaMemcpyAsync(dx, x, bytes, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) {
+        rc = ctx->op64.apply(dx, dy, conj != 0, ctx->stream, ctx->err);
+        if (!rc) {
+            e = cudaMemcpyAsync(y, dy, bytes, cudaMemcpyDeviceToHost, ctx->stream);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        }
+    }
+    if (e != cudaSuccess) rc = ctx->set_error(VIE_ERR_CUDA, cudaGetErrorString(e));
+    cudaFree(dx);
+    cudaFree(dy);
+    return rc;
+}
+
+int vie_solve(vie_ctx* ctx, const vie_solve_params* p, double* x, vie_solve_info* info) {
+    if (check_ctx(ctx) || !p) return VIE_ERR_ARG;
+    int rc = ready_for_operator(ctx);
+    if (rc) return rc;
+    if (!ctx->have_rhs) return ctx->set_error(VIE_ERR_STATE, "no right-hand side (vie_incident / vie_set_rhs)");
+    if (!(p->tol > 0)) return ctx->set_error(VIE_ERR_ARG, "tolerance must be positive");
+    cudaSetDevice(ctx->device);
+    ctx->err.code = VIE_OK;
+    ctx->err.msg.clear();
+    rc = solve_driver(ctx, p, info);
+    if (x && ctx->have_x) {
+        cudaError_t e = cudaMemcpyAsync(x, ctx->d_x, sizeof(double2) * 3 * (size_t)ctx->a, cudaMemcpyDeviceToHost,
+                                        ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess && !rc) rc = ctx->set_error(VIE_ERR_CUDA, cudaGetErrorString(e));
+    }
+    return rc;
+}
+
+int vie_get_solution(vie_ctx* ctx, double* x) {
+    if (check_ctx(ctx) || !x) return VIE_ERR_ARG;
+    if (!ctx->have_x) return ctx->set_error(VIE_ERR_STATE, "no solution yet (vie_solve)");
+    cudaSetDevice(ctx->device);
+    CTX_CUDA(cudaMemcpyAsync(x, ctx->d_x, sizeof(double2) * 3 * (size_t)ctx->a, cudaMemcpyDeviceToHost, ctx->stream));
+    CTX_CUDA(cudaStreamSynchronize(ctx->stream));
+    return VIE_OK;
+}
+
+int vie_solution_device(vie_ctx* ctx, const void** x) {
+    if (check_ctx(ctx) || !x) return VIE_ERR_ARG;
+    *x = ctx->d_x;
+    return VIE_OK;
+}
+
+int vie_stream(vie_ctx* ctx, void** stream) {
+    if (check_ctx(ctx) || !stream) return VIE_ERR_ARG;
+    *stream = (void*)ctx->stream;
+    return VIE_OK;
+}
+
+int vie_sync(vie_ctx* ctx) {
+    if (check_ctx(ctx)) return VIE_ERR_ARG;
+    CTX_CUDA(cudaStreamSynchronize(ctx->stream));
+    return VIE_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,118 @@
+// vie_internal.h -- host-side structures of the VIE library (not part of the ABI).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/vie_b200.h"
+#include "vie_operator.cuh"
+
+namespace vie {
+
+constexpr double kPI = 3.1415926535897932384626433832795;  // common.h:17
+constexpr double kZ0 = 120 * kPI;                            // common.h:18
+
+struct Error {
+    int code = VIE_OK;
+    std::string msg;
+};
+
+#define VIE_CUDA_TRY(expr, errobj)                                                        \
+    do {                                                                                  \
+        cudaError_t e__ = (expr);                                                         \
+        if (e__ != cudaSuccess) {                                                         \
+            (errobj).code = VIE_ERR_CUDA;                                                 \
+            (errobj).msg = std::string(#expr) + ": " + cudaGetErrorString(e__);          \
+            return VIE_ERR_CUDA;                                                          \
+        }                                                                                 \
+    } while (0)
+
+// Radix plan for a length-n transform; an empty override means the default
+// greedy factorisation (16, 8, 4, 2, 3, 5, 7, then any prime).
+AxisPlan make_axis_plan(int n, const std::vector<int>& override_radices = {});
+// DIF output position of every index (perm[m]) for a plan.
+std::vector<int> axis_perm(const AxisPlan& pl);
+
+// Tile sizes of the five passes for one precision.
+struct TileCfg {
+    int tz = 0, tc = 0, tx = 0;
+};
+
+// Operator state for one arithmetic precision.  Owns its tables, the Green
+// octant and per-voxel contrast in that precision, and the b/c scratch.
+template <typename T> struct Operator {
+    using C = cplx_t<T>;
+    bool ready = false;
+    OpDev<C> dev{};
+    size_t smem_z = 0, smem_y = 0, smem_x = 0;
+    // owned device allocations
+    void* d_tables = nullptr;
+    C* d_Gs = nullptr;
+    C* d_w = nullptr;
+    C* d_b = nullptr;
+    C* d_c = nullptr;
+    bool owns_scratch = true;
+
+    int init(int nx, int ny, int nz, const double d[3], double k0, const TileCfg& tiles,
+             const AxisPlan plans[3], const unsigned char* d_flags, Error& err);
+    // upload the Green octant (FP64, unscaled, on device) scaled by i Z0/(k0 M) in precision T
+    int set_green(const double2* d_oct64, double k0, cudaStream_t st, Error& err);
+    // per-voxel 1/(eps-1) from host doubles (interleaved complex)
+    int set_contrast(const double* w_host, cudaStream_t st, Error& err);
+    void release();
+    // y = A x (conj: A^H), plain store
+    int apply(const C* x, C* y, bool conj, cudaStream_t st, Error& err);
+    size_t scratch_bytes() const;
+};
+
+// Device-resident Krylov scalars (FP64 complex), one block per solve.
+enum ScalarSlot {
+    S_RHO = 0, S_RHO1, S_ALPHA, S_OMEGA, S_BETA, S_BNRM2, S_RR, S_ERR,
+    S_T0, S_T1, S_T2, S_T3, S_T4, S_T5, S_DONE, S_NAN, S_COUNT
+};
+
+}  // namespace vie
+
+// The opaque context of the C ABI.
+struct vie_ctx {
+    int device = 0;
+    int nx = 0, ny = 0, nz = 0;
+    long long a = 0;
+    double d[3] = {0, 0, 0};
+    double k0 = 0;
+    cudaStream_t stream = nullptr;
+    vie::Error err;
+
+    // geometry / material (device)
+    unsigned char* d_flags = nullptr;     // packed Flag_X | Flag_Y<<1 | Flag_Z<<2
+    std::vector<double> w_host;           // 1/(eps-1) per voxel, interleaved
+    bool have_flags = false, have_eps = false;
+
+    // Green octant (FP64, unscaled) and operators
+    double2* d_green = nullptr;           // (nx+1)(ny+1)(nz+1)
+    bool have_green = false;
+    vie::AxisPlan plans[3];
+    vie::Operator<double> op64;
+    vie::Operator<float> op32;
+
+    // right-hand side and solution (FP64, 3a each)
+    double2* d_rhs = nullptr;
+    double2* d_x = nullptr;
+    bool have_rhs = false, have_x = false;
+
+    // Krylov workspace (allocated on first solve)
+    std::vector<void*> work;
+    double2* d_scal = nullptr;            // vie::S_COUNT scalars
+    double2* d_partial = nullptr;         // reduction partials
+    size_t partial_cap = 0;               // entries
+    double2* h_scal = nullptr;            // pinned mirror
+
+    int set_error(int code, const std::string& m) {
+        err.code = code;
+        err.msg = m;
+        return code;
+    }
+};

@@ -1,0 +1,992 @@
+// vie_krylov.cu -- Krylov drivers of CG_Iteration.h on the GPU.
+//
+// All scalars (rho, alpha, omega, beta, norms) live in device memory as FP64
+// complex and are produced by one-block finalize kernels from per-block
+// partial sums (fixed summation order, so runs are deterministic).  Dot
+// products always accumulate in FP64, also when the vectors are FP32.  The
+// host only reads the error estimate once per iteration to decide whether to
+// stop, like the reference's printf/break (CG_Iteration.h:733-747).
+//
+// BiCGSTAB fuses its vector updates into the operator passes:
+//   p = r + beta (p - omega v)    in the first pass of A p  (CG_Iteration.h:611-633)
+//   b^H v                         in the last pass of A p   (:652-662)
+//   s = r - alpha v               in the first pass of A s  (:664-672)
+//   t^H s, t^H t                  in the last pass of A s   (:689-706)
+//   x += alpha p + omega s, r = s - omega t, r^H r, b^H r   one vector pass (:708-731, :594-598)
+#include <chrono>
+#include <cmath>
+#include <cstring>
+
+#include "vie_launch.cuh"
+
+namespace vie {
+
+// ---------------------------------------------------------------------------
+// device complex helpers on double2
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double2 ddiv(double2 a, double2 b) {
+    // Smith's scaled division
+    if (fabs(b.x) >= fabs(b.y)) {
+        const double r = b.y / b.x, d = b.x + b.y * r;
+        return make_double2((a.x + a.y * r) / d, (a.y - a.x * r) / d);
+    }
+    const double r = b.x / b.y, d = b.x * r + b.y;
+    return make_double2((a.x * r + a.y) / d, (a.y * r - a.x) / d);
+}
+__device__ __forceinline__ double2 dmul(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ bool dfinite(double2 a) { return isfinite(a.x) && isfinite(a.y); }
+
+template <typename C> __device__ __forceinline__ C coef_c(double2 v) { return from_d2<C>(v); }
+
+// conj(u) * v accumulated in FP64
+template <typename C> __device__ __forceinline__ void acc_dotc(double2& acc, C u, C v) {
+    const double ux = u.x, uy = u.y, vx = v.x, vy = v.y;
+    acc.x += ux * vx + uy * vy;
+    acc.y += ux * vy - uy * vx;
+}
+template <typename C> __device__ __forceinline__ void acc_dotu(double2& acc, C u, C v) {
+    const double ux = u.x, uy = u.y, vx = v.x, vy = v.y;
+    acc.x += ux * vx - uy * vy;
+    acc.y += ux * vy + uy * vx;
+}
+
+// ---------------------------------------------------------------------------
+// finalize: fixed-order sum of the partials, then a scalar update on thread 0
+// ---------------------------------------------------------------------------
+template <int K, class Fin>
+__global__ void __launch_bounds__(256) k_finalize(const double2* __restrict__ partial, long long nblk, double2* S,
+                                                  Fin fin) {
+    __shared__ double2 red[K][256];
+    for (int k = 0; k < K; k++) {
+        double rx = 0, ry = 0;
+        for (long long b = threadIdx.x; b < nblk; b += blockDim.x) {
+            const double2 v = partial[b * K + k];
+            rx += v.x;
+            ry += v.y;
+        }
+        red[k][threadIdx.x] = make_double2(rx, ry);
+    }
+    __syncthreads();
+    for (int h = 128; h > 0; h >>= 1) {
+        if (threadIdx.x < h)
+            for (int k = 0; k < K; k++) {
+                red[k][threadIdx.x].x += red[k][threadIdx.x + h].x;
+                red[k][threadIdx.x].y += red[k][threadIdx.x + h].y;
+            }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        double2 d[K];
+        for (int k = 0; k < K; k++) d[k] = red[k][0];
+        fin(S, d);
+    }
+}
+
+// scalar programs -----------------------------------------------------------
+struct FinStore1 {  // S[slot] = d0
+    int slot;
+    __device__ void operator()(double2* S, const double2* d) const { S[slot] = d[0]; }
+};
+struct FinStore2 {
+    int s0, s1;
+    __device__ void operator()(double2* S, const double2* d) const { S[s0] = d[0]; S[s1] = d[1]; }
+};
+// BiCGSTAB -------------------------------------------------------------------
+struct FinBicgstabInit {  // d0 = b^H b, d1 = b^H r
+    __device__ void operator()(double2* S, const double2* d) const {
+        S[S_BNRM2] = d[0];
+        S[S_RHO] = d[1];
+        S[S_OMEGA] = make_double2(1.0, 0.0);  // :587-588
+        S[S_ALPHA] = make_double2(0.0, 0.0);
+        S[S_NAN] = make_double2(0.0, 0.0);
+    }
+};
+struct FinAlpha {  // alpha = rho / d0
+    __device__ void operator()(double2* S, const double2* d) const {
+        S[S_ALPHA] = ddiv(S[S_RHO], d[0]);
+        if (!dfinite(S[S_ALPHA])) S[S_NAN] = make_double2(1.0, 0.0);
+    }
+};
+struct FinOmega {  // omega = (t^H s) / (t^H t)
+    __device__ void operator()(double2* S, const double2* d) const {
+        S[S_OMEGA] = ddiv(d[0], d[1]);
+        if (!dfinite(S[S_OMEGA])) S[S_NAN] = make_double2(1.0, 0.0);
+    }
+};
+struct FinBicgstabUpdate {  // d0 = r^H r, d1 = b^H r(new)
+    __device__ void operator()(double2* S, const double2* d) const {
+        S[S_RR] = d[0];
+        S[S_ERR] = make_double2(sqrt(d[0].x / S[S_BNRM2].x), 0.0);  // :734
+        const double2 rho_new = d[1];
+        // beta = (rho / rho_1) (alpha / omega)  (:603-609), for the next iteration
+        S[S_BETA] = dmul(ddiv(rho_new, S[S_RHO]), ddiv(S[S_ALPHA], S[S_OMEGA]));
+        S[S_RHO1] = S[S_RHO];
+        S[S_RHO] = rho_new;
+        if (!dfinite(S[S_ERR]) || !dfinite(S[S_BETA])) S[S_NAN] = make_double2(1.0, 0.0);
+    }
+};
+// CORS -----------------------------------------------------------------------
+struct FinCorsRho {  // d0 = b^H A r
+    int first;
+    __device__ void operator()(double2* S, const double2* d) const {
+        S[S_RHO] = d[0];
+        if (!first) {
+            const double2 beta = ddiv(d[0], S[S_RHO1]);  // :874-878
+            S[S_BETA] = beta;
+            S[S_T0] = dmul(beta, beta);
+        }
+        if (!dfinite(S[S_RHO]) || !dfinite(S[S_BETA])) S[S_NAN] = make_double2(1.0, 0.0);
+    }
+};
+struct FinCorsAlpha {  // d0 = b^H A q
+    __device__ void operator()(double2* S, const double2* d) const {
+        const double2 al = ddiv(S[S_RHO], d[0]);  // :951-962
+        S[S_ALPHA] = al;
+        S[S_T1] = dmul(al, al);
+        if (!dfinite(al)) S[S_NAN] = make_double2(1.0, 0.0);
+    }
+};
+struct FinErr {  // d0 = r^H r; err = sqrt(rr / bnrm2); rho_1 = rho
+    __device__ void operator()(double2* S, const double2* d) const {
+        S[S_RR] = d[0];
+        S[S_ERR] = make_double2(sqrt(d[0].x / S[S_BNRM2].x), 0.0);
+        S[S_RHO1] = S[S_RHO];
+        if (!dfinite(S[S_ERR])) S[S_NAN] = make_double2(1.0, 0.0);
+    }
+};
+// BiCORSTAB ------------------------------------------------------------------
+struct FinBicorRho {  // d0 = b^H A r
+    int first;
+    __device__ void operator()(double2* S, const double2* d) const {
+        S[S_RHO] = d[0];
+        if (!first) {
+            S[S_BETA] = dmul(ddiv(d[0], S[S_RHO1]), ddiv(S[S_ALPHA], S[S_OMEGA]));  // :1167-1173
+            S[S_T2] = dmul(S[S_BETA], S[S_OMEGA]);  // beta * omega of the previous step
+        }
+        if (!dfinite(S[S_RHO]) || !dfinite(S[S_BETA])) S[S_NAN] = make_double2(1.0, 0.0);
+    }
+};
+struct FinBicorOmega {  // S_T3 = conj(pc)^T qc, S_T4 = qc^H qc  ->  omega = conj(S_T3) / S_T4
+    __device__ void operator()(double2* S, const double2* d) const {
+        const double2 num = make_double2(d[0].x, -d[0].y);
+        S[S_OMEGA] = ddiv(num, d[1]);
+        if (!dfinite(S[S_OMEGA])) S[S_NAN] = make_double2(1.0, 0.0);
+    }
+};
+// CG (CGNR) ------------------------------------------------------------------
+struct FinCgInit {  // d0 = ||p||^2 (v3), d1 = ||b||^2 (vx)
+    __device__ void operator()(double2* S, const double2* d) const {
+        S[S_T0] = d[0];
+        S[S_BNRM2] = d[1];
+        S[S_NAN] = make_double2(0.0, 0.0);
+    }
+};
+struct FinCgAlpha {  // d0 = ||Ap||^2 (v2); alpha = v1 / v2 with v1 = v3
+    __device__ void operator()(double2* S, const double2* d) const {
+        S[S_T1] = S[S_T0];  // v1 = v3
+        S[S_ALPHA] = make_double2(S[S_T1].x / d[0].x, 0.0);
+        if (!dfinite(S[S_ALPHA])) S[S_NAN] = make_double2(1.0, 0.0);
+    }
+};
+struct FinCgBeta {  // d0 = ||q||^2 (v3); beta = v3 / v1
+    __device__ void operator()(double2* S, const double2* d) const {
+        S[S_T0] = d[0];
+        S[S_BETA] = make_double2(d[0].x / S[S_T1].x, 0.0);
+        if (!dfinite(S[S_BETA])) S[S_NAN] = make_double2(1.0, 0.0);
+    }
+};
+struct FinCgErr {  // d0 = ||r||^2 (v4); err = v4 / vx (not rooted, :323)
+    __device__ void operator()(double2* S, const double2* d) const {
+        S[S_RR] = d[0];
+        S[S_ERR] = make_double2(d[0].x / S[S_BNRM2].x, 0.0);
+        if (!dfinite(S[S_ERR])) S[S_NAN] = make_double2(1.0, 0.0);
+    }
+};
+// BiCG -------------------------------------------------------------------------
+struct FinBicgInit {  // d0 = r^T r
+    __device__ void operator()(double2* S, const double2* d) const {
+        S[S_BNRM2] = d[0];  // vx
+        S[S_T0] = ddiv(make_double2(1.0, 0.0), d[0]);  // 1/v1
+        S[S_NAN] = make_double2(0.0, 0.0);
+    }
+};
+struct FinBicgAlpha {  // d0 = Ap^T p; alpha = 1/v1
+    __device__ void operator()(double2* S, const double2* d) const {
+        S[S_ALPHA] = ddiv(make_double2(1.0, 0.0), d[0]);
+        if (!dfinite(S[S_ALPHA])) S[S_NAN] = make_double2(1.0, 0.0);
+    }
+};
+struct FinBicgBeta {  // d0 = r^T r (v2); beta = 1/v2; err = sqrt(|v2|^2/|vx|^2)
+    __device__ void operator()(double2* S, const double2* d) const {
+        const double2 v2 = d[0], vx = S[S_BNRM2];
+        S[S_BETA] = ddiv(make_double2(1.0, 0.0), v2);
+        S[S_ERR] = make_double2(sqrt((v2.x * v2.x + v2.y * v2.y) / (vx.x * vx.x + vx.y * vx.y)), 0.0);
+        if (!dfinite(S[S_ERR]) || !dfinite(S[S_BETA])) S[S_NAN] = make_double2(1.0, 0.0);
+    }
+};
+// refinement -------------------------------------------------------------------
+struct FinNorm {  // S[slot] = d0 (a squared norm)
+    int slot;
+    __device__ void operator()(double2* S, const double2* d) const { S[slot] = d[0]; }
+};
+
+// ---------------------------------------------------------------------------
+// generic fused vector kernel:  y = sum_i c_i x_i  (+ y if acc), c_i from slots;
+// optional dots conj(u_k) . y_new (or plain u_k . y_new)
+// ---------------------------------------------------------------------------
+struct CoefSpec {
+    int slot;       // -1: constant
+    double re, im;  // multiplier
+};
+template <typename C> struct LinTerm {
+    const C* x;
+    CoefSpec c;
+};
+template <typename C> struct DotSpec {
+    const C* u;  // nullptr: u = y_new
+    int conj;
+};
+template <typename C, int NT, int K> struct LinArgs {
+    C* y;
+    int acc;
+    LinTerm<C> t[NT];
+    DotSpec<C> d[K > 0 ? K : 1];
+};
+
+__device__ __forceinline__ double2 eval_coef(const CoefSpec& c, const double2* S) {
+    const double2 base = c.slot >= 0 ? S[c.slot] : make_double2(1.0, 0.0);
+    return dmul(base, make_double2(c.re, c.im));
+}
+
+template <typename C, int NT, int K>
+__global__ void __launch_bounds__(256) k_lin(LinArgs<C, NT, K> g, long long n, const double2* __restrict__ S,
+                                             double2* __restrict__ partial) {
+    C cf[NT];
+#pragma unroll
+    for (int i = 0; i < NT; i++) cf[i] = coef_c<C>(eval_coef(g.t[i].c, S));
+    constexpr int KA = K > 0 ? K : 1;
+    double2 acc[KA];
+#pragma unroll
+    for (int k = 0; k < KA; k++) acc[k] = make_double2(0, 0);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        C v = g.acc ? g.y[i] : czero<C>();
+#pragma unroll
+        for (int t = 0; t < NT; t++) v = cadd(v, cmul(cf[t], g.t[t].x[i]));
+        g.y[i] = v;
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            const C u = g.d[k].u ? g.d[k].u[i] : v;
+            if (g.d[k].conj) acc_dotc(acc[k], u, v);
+            else acc_dotu(acc[k], u, v);
+        }
+    }
+    if constexpr (K > 0) block_reduce_store<KA>(acc, partial, blockIdx.x);
+}
+
+// dots only
+template <typename C, int K> struct DotArgs {
+    const C* u[K];
+    const C* v[K];
+    int conj[K];
+};
+template <typename C, int K>
+__global__ void __launch_bounds__(256) k_dots(DotArgs<C, K> g, long long n, double2* __restrict__ partial) {
+    double2 acc[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) acc[k] = make_double2(0, 0);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            if (g.conj[k]) acc_dotc(acc[k], g.u[k][i], g.v[k][i]);
+            else acc_dotu(acc[k], g.u[k][i], g.v[k][i]);
+        }
+    }
+    block_reduce_store<K>(acc, partial, blockIdx.x);
+}
+
+// b = e . flag (Current_Reset on E_inc, CG_Iteration.h:560-562), converted to C
+template <typename C>
+__global__ void k_mask_rhs(const double2* __restrict__ e, const unsigned char* __restrict__ flags, C* __restrict__ b,
+                           long long a, double scale) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < 3 * a;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int s = (int)(i / a);
+        const long long v = i - s * a;
+        const double f = ((flags[v] >> s) & 1) ? scale : 0.0;
+        b[i] = from_d2<C>(make_double2(e[i].x * f, e[i].y * f));
+    }
+}
+
+// y64 (+)= scale * x (C precision)
+template <typename C>
+__global__ void k_accum_d(double2* __restrict__ y, const C* __restrict__ x, long long n, const double2* S, int slot,
+                          int accumulate) {
+    const double s = slot >= 0 ? sqrt(S[slot].x) : 1.0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const double2 v = as_d2(x[i]);
+        double2 o = accumulate ? y[i] : make_double2(0, 0);
+        o.x += s * v.x;
+        o.y += s * v.y;
+        y[i] = o;
+    }
+}
+
+// y32 = x64 / sqrt(S[slot])
+template <typename C>
+__global__ void k_scale_to(C* __restrict__ y, const double2* __restrict__ x, long long n, const double2* S, int slot) {
+    const double s = 1.0 / sqrt(S[slot].x);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        y[i] = from_d2<C>(make_double2(x[i].x * s, x[i].y * s));
+}
+
+// ---------------------------------------------------------------------------
+// prologue / epilogue functors of the fused BiCGSTAB and refinement
+// ---------------------------------------------------------------------------
+template <typename C> struct ProCopyWrite {  // p = r
+    const C* __restrict__ r;
+    C* __restrict__ p;
+    long long a;
+    __device__ __forceinline__ C operator()(int s, long long idx, bool) const {
+        const C v = r[s * a + idx];
+        p[s * a + idx] = v;
+        return v;
+    }
+};
+template <typename C> struct ProBicgP {  // p = r + beta (p - omega v)
+    const C* __restrict__ r;
+    C* __restrict__ p;
+    const C* __restrict__ v;
+    const double2* __restrict__ S;
+    long long a;
+    __device__ __forceinline__ C operator()(int s, long long idx, bool) const {
+        const C beta = from_d2<C>(S[S_BETA]), omega = from_d2<C>(S[S_OMEGA]);
+        const long long o = s * a + idx;
+        const C pv = cadd(r[o], cmul(beta, csub(p[o], cmul(omega, v[o]))));
+        p[o] = pv;
+        return pv;
+    }
+};
+template <typename C> struct ProBicgS {  // s = r - alpha v
+    const C* __restrict__ r;
+    const C* __restrict__ v;
+    C* __restrict__ sv;
+    const double2* __restrict__ S;
+    long long a;
+    __device__ __forceinline__ C operator()(int s, long long idx, bool) const {
+        const C alpha = from_d2<C>(S[S_ALPHA]);
+        const long long o = s * a + idx;
+        const C x = csub(r[o], cmul(alpha, v[o]));
+        sv[o] = x;
+        return x;
+    }
+};
+template <typename C> struct EpiDotB {  // store y; acc conj(b) y
+    static constexpr int K = 1;
+    C* __restrict__ y;
+    const C* __restrict__ b;
+    long long a;
+    __device__ __forceinline__ void operator()(int s, long long idx, C v, double2* acc) const {
+        const long long o = s * a + idx;
+        y[o] = v;
+        acc_dotc(acc[0], b[o], v);
+    }
+};
+template <typename C> struct EpiDotTS {  // store t; acc conj(t) s, conj(t) t
+    static constexpr int K = 2;
+    C* __restrict__ y;
+    const C* __restrict__ sv;
+    long long a;
+    __device__ __forceinline__ void operator()(int s, long long idx, C v, double2* acc) const {
+        const long long o = s * a + idx;
+        y[o] = v;
+        acc_dotc(acc[0], v, sv[o]);
+        acc_dotc(acc[1], v, v);
+    }
+};
+template <typename C> struct EpiNorm {  // store y; acc ||y||^2
+    static constexpr int K = 1;
+    C* __restrict__ y;
+    long long a;
+    __device__ __forceinline__ void operator()(int s, long long idx, C v, double2* acc) const {
+        y[s * a + idx] = v;
+        acc_dotc(acc[0], v, v);
+    }
+};
+template <typename C> struct EpiDotU {  // store y; acc y^T u (unconjugated)
+    static constexpr int K = 1;
+    C* __restrict__ y;
+    const C* __restrict__ u;
+    long long a;
+    __device__ __forceinline__ void operator()(int s, long long idx, C v, double2* acc) const {
+        const long long o = s * a + idx;
+        y[o] = v;
+        acc_dotu(acc[0], v, u[o]);
+    }
+};
+template <typename C> struct EpiResidual {  // r = b - y; acc ||r||^2
+    static constexpr int K = 1;
+    C* __restrict__ r;
+    const C* __restrict__ b;
+    long long a;
+    __device__ __forceinline__ void operator()(int s, long long idx, C v, double2* acc) const {
+        const long long o = s * a + idx;
+        const C rv = csub(b[o], v);
+        r[o] = rv;
+        acc_dotc(acc[0], rv, rv);
+    }
+};
+
+// x += alpha p + omega s; r = s - omega t; acc r^H r, b^H r
+template <typename C>
+__global__ void __launch_bounds__(256) k_bicgstab_update(C* __restrict__ x, const C* __restrict__ p,
+                                                         const C* __restrict__ sv, const C* __restrict__ t,
+                                                         C* __restrict__ r, const C* __restrict__ b, long long n,
+                                                         const double2* __restrict__ S, double2* __restrict__ partial) {
+    const C alpha = from_d2<C>(S[S_ALPHA]), omega = from_d2<C>(S[S_OMEGA]);
+    double2 acc[2] = {make_double2(0, 0), make_double2(0, 0)};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const C si = sv[i];
+        x[i] = cadd(cadd(x[i], cmul(alpha, p[i])), cmul(omega, si));
+        const C ri = csub(si, cmul(omega, t[i]));
+        r[i] = ri;
+        acc_dotc(acc[0], ri, ri);
+        acc_dotc(acc[1], b[i], ri);
+    }
+    block_reduce_store<2>(acc, partial, blockIdx.x);
+}
+
+// ---------------------------------------------------------------------------
+// workspace helpers
+// ---------------------------------------------------------------------------
+constexpr int kVecBlocks = 148 * 8;
+
+static int ensure_scalars(vie_ctx* ctx) {
+    if (!ctx->d_scal) {
+        VIE_CUDA_TRY(cudaMalloc(&ctx->d_scal, sizeof(double2) * S_COUNT * 4), ctx->err);
+        VIE_CUDA_TRY(cudaMallocHost(&ctx->h_scal, sizeof(double2) * S_COUNT), ctx->err);
+    }
+    const long long need = std::max<long long>(kVecBlocks, 3LL * ((long long)ctx->nx * ctx->ny + 1)) * 4;
+    if ((long long)ctx->partial_cap < need) {
+        if (ctx->d_partial) cudaFree(ctx->d_partial);
+        VIE_CUDA_TRY(cudaMalloc(&ctx->d_partial, sizeof(double2) * need), ctx->err);
+        ctx->partial_cap = need;
+    }
+    return VIE_OK;
+}
+
+// pool of 3a-vectors by byte size
+static void* work_vec(vie_ctx* ctx, int idx, size_t elem, int* rc) {
+    const size_t bytes = elem * 3 * (size_t)ctx->a;
+    // slot layout: ctx->work holds pairs (ptr, size) encoded as two entries
+    const size_t need = 2 * (size_t)(idx + 1);
+    while (ctx->work.size() < need) ctx->work.push_back(nullptr);
+    void*& p = ctx->work[2 * idx];
+    size_t sz = (size_t)(uintptr_t)ctx->work[2 * idx + 1];
+    if (p && sz >= bytes) return p;
+    if (p) cudaFree(p);
+    p = nullptr;
+    if (cudaMalloc(&p, bytes) != cudaSuccess) {
+        *rc = ctx->set_error(VIE_ERR_ALLOC, "device allocation of a Krylov vector failed");
+        ctx->work[2 * idx + 1] = nullptr;
+        return nullptr;
+    }
+    ctx->work[2 * idx + 1] = (void*)(uintptr_t)bytes;
+    return p;
+}
+
+template <int K, class Fin>
+static int finalize(vie_ctx* ctx, long long nblk, Fin fin) {
+    k_finalize<K, Fin><<<1, 256, 0, ctx->stream>>>(ctx->d_partial, nblk, ctx->d_scal, fin);
+    VIE_CUDA_TRY(cudaGetLastError(), ctx->err);
+    return VIE_OK;
+}
+
+template <typename C, int NT, int K>
+static int lin(vie_ctx* ctx, const LinArgs<C, NT, K>& g) {
+    k_lin<C, NT, K><<<kVecBlocks, 256, 0, ctx->stream>>>(g, 3 * ctx->a, ctx->d_scal, ctx->d_partial);
+    VIE_CUDA_TRY(cudaGetLastError(), ctx->err);
+    return VIE_OK;
+}
+
+template <typename C, int K>
+static int dots(vie_ctx* ctx, const DotArgs<C, K>& g) {
+    k_dots<C, K><<<kVecBlocks, 256, 0, ctx->stream>>>(g, 3 * ctx->a, ctx->d_partial);
+    VIE_CUDA_TRY(cudaGetLastError(), ctx->err);
+    return VIE_OK;
+}
+
+static CoefSpec cs(int slot, double re = 1.0, double im = 0.0) { return CoefSpec{slot, re, im}; }
+
+// read err and nan flags
+static int read_scalars(vie_ctx* ctx) {
+    VIE_CUDA_TRY(cudaMemcpyAsync(ctx->h_scal, ctx->d_scal, sizeof(double2) * S_COUNT, cudaMemcpyDeviceToHost,
+                                 ctx->stream),
+                 ctx->err);
+    VIE_CUDA_TRY(cudaStreamSynchronize(ctx->stream), ctx->err);
+    return VIE_OK;
+}
+
+struct KrylovResult {
+    int steps = -1;
+    int iterations = 0;
+    int matvecs = 0;
+    double err = -1;
+    int status = VIE_OK;
+};
+
+// matvec with generic prologue/epilogue on operator op
+template <typename T, class Pro, class Epi>
+static int opmv(vie_ctx* ctx, Operator<T>& op, Pro pro, Epi epi, const cplx_t<T>* xdiag, bool conj) {
+    return launch_operator<T>(op, pro, epi, xdiag, conj, ctx->d_partial, ctx->stream, ctx->err);
+}
+
+// ---------------------------------------------------------------------------
+// solvers on C-precision vectors.  b: masked right-hand side, x: solution
+// (zeroed here), thr: threshold on the solver's own error measure.
+// ---------------------------------------------------------------------------
+template <typename T>
+static int solve_bicgstab(vie_ctx* ctx, Operator<T>& op, const cplx_t<T>* b, cplx_t<T>* x, double thr, int maxit,
+                          int verbose, int vbase, KrylovResult& res) {
+    using C = cplx_t<T>;
+    int rc = VIE_OK;
+    const long long a = ctx->a, n = 3 * a;
+    C* r = (C*)work_vec(ctx, vbase + 0, sizeof(C), &rc);
+    C* p = (C*)work_vec(ctx, vbase + 1, sizeof(C), &rc);
+    C* v = (C*)work_vec(ctx, vbase + 2, sizeof(C), &rc);
+    C* sv = (C*)work_vec(ctx, vbase + 3, sizeof(C), &rc);
+    C* t = (C*)work_vec(ctx, vbase + 4, sizeof(C), &rc);
+    if (rc) return rc;
+    cudaStream_t st = ctx->stream;
+    VIE_CUDA_TRY(cudaMemsetAsync(x, 0, sizeof(C) * n, st), ctx->err);
+    VIE_CUDA_TRY(cudaMemcpyAsync(r, b, sizeof(C) * n, cudaMemcpyDeviceToDevice, st), ctx->err);  // :565-567
+    {
+        DotArgs<C, 2> g{{b, b}, {b, r}, {1, 1}};
+        if ((rc = dots(ctx, g))) return rc;
+        if ((rc = finalize<2>(ctx, kVecBlocks, FinBicgstabInit{}))) return rc;
+    }
+    const long long nblk = epilogue_blocks(op);
+    for (int m = 0; m < maxit; m++) {
+        if (m == 0) {
+            if ((rc = opmv(ctx, op, ProCopyWrite<C>{r, p, a}, EpiDotB<C>{v, b, a}, p, false))) return rc;
+        } else {
+            if ((rc = opmv(ctx, op, ProBicgP<C>{r, p, v, ctx->d_scal, a}, EpiDotB<C>{v, b, a}, p, false))) return rc;
+        }
+        if ((rc = finalize<1>(ctx, nblk, FinAlpha{}))) return rc;
+        if ((rc = opmv(ctx, op, ProBicgS<C>{r, v, sv, ctx->d_scal, a}, EpiDotTS<C>{t, sv, a}, sv, false))) return rc;
+        if ((rc = finalize<2>(ctx, nblk, FinOmega{}))) return rc;
+        k_bicgstab_update<C><<<kVecBlocks, 256, 0, st>>>(x, p, sv, t, r, b, n, ctx->d_scal, ctx->d_partial);
+        VIE_CUDA_TRY(cudaGetLastError(), ctx->err);
+        if ((rc = finalize<2>(ctx, kVecBlocks, FinBicgstabUpdate{}))) return rc;
+        res.matvecs += 2;
+        res.iterations = m + 1;
+        if ((rc = read_scalars(ctx))) return rc;
+        const double err = ctx->h_scal[S_ERR].x;
+        res.err = err;
+        if (ctx->h_scal[S_NAN].x != 0.0) {
+            if (err < thr) { res.steps = m; return VIE_OK; }
+            res.status = VIE_ERR_BREAKDOWN;
+            return ctx->set_error(VIE_ERR_BREAKDOWN, "BiCGSTAB breakdown (zero or non-finite scalar) at step " +
+                                                         std::to_string(m));
+        }
+        if (err < thr) {
+            if (verbose) printf("CG Error: %lf\nSteps: %d\n\n", err, m);
+            res.steps = m;
+            return VIE_OK;
+        }
+        if (verbose) printf("CG Error: %lf\n", err);
+    }
+    res.status = VIE_ERR_MAXIT;
+    return VIE_OK;
+}
+
+template <typename T>
+static int solve_cors(vie_ctx* ctx, Operator<T>& op, const cplx_t<T>* b, cplx_t<T>* x, double thr, int maxit,
+                      int verbose, int vbase, KrylovResult& res) {
+    using C = cplx_t<T>;
+    int rc = VIE_OK;
+    const long long a = ctx->a, n = 3 * a;
+    C* r = (C*)work_vec(ctx, vbase + 0, sizeof(C), &rc);
+    C* p = (C*)work_vec(ctx, vbase + 1, sizeof(C), &rc);
+    C* q = (C*)work_vec(ctx, vbase + 2, sizeof(C), &rc);
+    C* Ap = (C*)work_vec(ctx, vbase + 3, sizeof(C), &rc);
+    C* Aq = (C*)work_vec(ctx, vbase + 4, sizeof(C), &rc);
+    C* rc_ = (C*)work_vec(ctx, vbase + 5, sizeof(C), &rc);
+    C* pc = (C*)work_vec(ctx, vbase + 6, sizeof(C), &rc);
+    C* qc = (C*)work_vec(ctx, vbase + 7, sizeof(C), &rc);
+    if (rc) return rc;
+    cudaStream_t st = ctx->stream;
+    VIE_CUDA_TRY(cudaMemsetAsync(x, 0, sizeof(C) * n, st), ctx->err);
+    VIE_CUDA_TRY(cudaMemcpyAsync(r, b, sizeof(C) * n, cudaMemcpyDeviceToDevice, st), ctx->err);  // :826-828
+    {
+        DotArgs<C, 1> g{{b}, {b}, {1}};
+        if ((rc = dots(ctx, g))) return rc;
+        if ((rc = finalize<1>(ctx, kVecBlocks, FinStore1{S_BNRM2}))) return rc;
+    }
+    const long long nblk = epilogue_blocks(op);
+    for (int m = 0; m < maxit; m++) {
+        // Ap = A r; rho = b^H Ap (:853-869)
+        if ((rc = opmv(ctx, op, ProCopy<C>{r, a}, EpiDotB<C>{Ap, b, a}, r, false))) return rc;
+        if ((rc = finalize<1>(ctx, nblk, FinCorsRho{m == 0}))) return rc;
+        if (m > 0) {
+            // p = r + beta pc; qc = Ap + beta rc; q = qc + beta rc + beta^2 q  (:880-915)
+            if ((rc = lin(ctx, LinArgs<C, 2, 0>{p, 0, {{r, cs(-1)}, {pc, cs(S_BETA)}}, {}}))) return rc;
+            if ((rc = lin(ctx, LinArgs<C, 2, 0>{qc, 0, {{Ap, cs(-1)}, {rc_, cs(S_BETA)}}, {}}))) return rc;
+            if ((rc = lin(ctx, LinArgs<C, 3, 0>{q, 0, {{q, cs(S_T0)}, {rc_, cs(S_BETA)}, {qc, cs(-1)}}, {}}))) return rc;
+        } else {
+            VIE_CUDA_TRY(cudaMemcpyAsync(p, r, sizeof(C) * n, cudaMemcpyDeviceToDevice, st), ctx->err);
+            VIE_CUDA_TRY(cudaMemcpyAsync(qc, Ap, sizeof(C) * n, cudaMemcpyDeviceToDevice, st), ctx->err);
+            VIE_CUDA_TRY(cudaMemcpyAsync(q, Ap, sizeof(C) * n, cudaMemcpyDeviceToDevice, st), ctx->err);
+        }
+        // Aq = A q; alpha = rho / (b^H Aq) (:938-962)
+        if ((rc = opmv(ctx, op, ProCopy<C>{q, a}, EpiDotB<C>{Aq, b, a}, q, false))) return rc;
+        if ((rc = finalize<1>(ctx, nblk, FinCorsAlpha{}))) return rc;
+        // pc = p - alpha q; rc = qc - alpha Aq (:964-981)
+        if ((rc = lin(ctx, LinArgs<C, 2, 0>{pc, 0, {{p, cs(-1)}, {q, cs(S_ALPHA, -1.0)}}, {}}))) return rc;
+        if ((rc = lin(ctx, LinArgs<C, 2, 0>{rc_, 0, {{qc, cs(-1)}, {Aq, cs(S_ALPHA, -1.0)}}, {}}))) return rc;
+        // x += 2 alpha p - alpha^2 q (:983-997); r += -2 alpha qc + alpha^2 Aq (:999-1012); r^H r
+        if ((rc = lin(ctx, LinArgs<C, 2, 0>{x, 1, {{p, cs(S_ALPHA, 2.0)}, {q, cs(S_T1, -1.0)}}, {}}))) return rc;
+        if ((rc = lin(ctx, LinArgs<C, 2, 1>{r, 1, {{qc, cs(S_ALPHA, -2.0)}, {Aq, cs(S_T1)}}, {{nullptr, 1}}})))
+            return rc;
+        if ((rc = finalize<1>(ctx, kVecBlocks, FinErr{}))) return rc;
+        res.matvecs += 2;
+        res.iterations = m + 1;
+        if ((rc = read_scalars(ctx))) return rc;
+        const double err = ctx->h_scal[S_ERR].x;
+        res.err = err;
+        if (ctx->h_scal[S_NAN].x != 0.0 && !(err < thr)) {
+            res.status = VIE_ERR_BREAKDOWN;
+            return ctx->set_error(VIE_ERR_BREAKDOWN, "CORS breakdown at step " + std::to_string(m));
+        }
+        if (err < thr) {
+            if (verbose) printf("CG Error: %lf\nSteps: %d\n\n", err, m);
+            res.steps = m;
+            return VIE_OK;
+        }
+        if (verbose) printf("CG Error: %lf\n", err);
+    }
+    res.status = VIE_ERR_MAXIT;
+    return VIE_OK;
+}
+
+template <typename T>
+static int solve_bicorstab(vie_ctx* ctx, Operator<T>& op, const cplx_t<T>* b, cplx_t<T>* x, double thr, int maxit,
+                           int verbose, int vbase, KrylovResult& res) {
+    using C = cplx_t<T>;
+    int rc = VIE_OK;
+    const long long a = ctx->a, n = 3 * a;
+    C* r = (C*)work_vec(ctx, vbase + 0, sizeof(C), &rc);
+    C* p = (C*)work_vec(ctx, vbase + 1, sizeof(C), &rc);
+    C* q = (C*)work_vec(ctx, vbase + 2, sizeof(C), &rc);
+    C* Ap = (C*)work_vec(ctx, vbase + 3, sizeof(C), &rc);
+    C* Aq = (C*)work_vec(ctx, vbase + 4, sizeof(C), &rc);
+    C* pc = (C*)work_vec(ctx, vbase + 5, sizeof(C), &rc);
+    C* qc = (C*)work_vec(ctx, vbase + 6, sizeof(C), &rc);
+    if (rc) return rc;
+    cudaStream_t st = ctx->stream;
+    VIE_CUDA_TRY(cudaMemsetAsync(x, 0, sizeof(C) * n, st), ctx->err);
+    VIE_CUDA_TRY(cudaMemcpyAsync(r, b, sizeof(C) * n, cudaMemcpyDeviceToDevice, st), ctx->err);  // :1118-1120
+    {
+        DotArgs<C, 1> g{{b}, {b}, {1}};
+        if ((rc = dots(ctx, g))) return rc;
+        if ((rc = finalize<1>(ctx, kVecBlocks, FinStore1{S_BNRM2}))) return rc;
+    }
+    const long long nblk = epilogue_blocks(op);
+    for (int m = 0; m < maxit; m++) {
+        if ((rc = opmv(ctx, op, ProCopy<C>{r, a}, EpiDotB<C>{Ap, b, a}, r, false))) return rc;   // :1145-1162
+        if ((rc = finalize<1>(ctx, nblk, FinBicorRho{m == 0}))) return rc;
+        if (m > 0) {
+            // p = r + beta (p - omega q); q = Ap + beta (q - omega Aq)  (:1175-1207)
+            if ((rc = lin(ctx, LinArgs<C, 3, 0>{p, 0, {{p, cs(S_BETA)}, {q, cs(S_T2, -1.0)}, {r, cs(-1)}}, {}})))
+                return rc;
+            if ((rc = lin(ctx, LinArgs<C, 3, 0>{q, 0, {{q, cs(S_BETA)}, {Aq, cs(S_T2, -1.0)}, {Ap, cs(-1)}}, {}})))
+                return rc;
+        } else {
+            VIE_CUDA_TRY(cudaMemcpyAsync(p, r, sizeof(C) * n, cudaMemcpyDeviceToDevice, st), ctx->err);
+            VIE_CUDA_TRY(cudaMemcpyAsync(q, Ap, sizeof(C) * n, cudaMemcpyDeviceToDevice, st), ctx->err);
+        }
+        if ((rc = opmv(ctx, op, ProCopy<C>{q, a}, EpiDotB<C>{Aq, b, a}, q, false))) return rc;   // :1224-1248
+        if ((rc = finalize<1>(ctx, nblk, FinAlpha{}))) return rc;
+        // pc = r - alpha q; qc = Ap - alpha Aq; omega = qc^H pc / qc^H qc  (:1250-1287)
+        if ((rc = lin(ctx, LinArgs<C, 2, 0>{pc, 0, {{r, cs(-1)}, {q, cs(S_ALPHA, -1.0)}}, {}}))) return rc;
+        if ((rc = lin(ctx, LinArgs<C, 2, 2>{qc, 0, {{Ap, cs(-1)}, {Aq, cs(S_ALPHA, -1.0)}}, {{pc, 1}, {nullptr, 1}}})))
+            return rc;
+        // d0 = conj(pc).qc, so qc^H pc = conj(d0)
+        if ((rc = finalize<2>(ctx, kVecBlocks, FinBicorOmega{}))) return rc;
+        // x += alpha p + omega pc; r = pc - omega qc; r^H r  (:1289-1315)
+        if ((rc = lin(ctx, LinArgs<C, 2, 0>{x, 1, {{p, cs(S_ALPHA)}, {pc, cs(S_OMEGA)}}, {}}))) return rc;
+        if ((rc = lin(ctx, LinArgs<C, 2, 1>{r, 0, {{pc, cs(-1)}, {qc, cs(S_OMEGA, -1.0)}}, {{nullptr, 1}}}))) return rc;
+        if ((rc = finalize<1>(ctx, kVecBlocks, FinErr{}))) return rc;
+        res.matvecs += 2;
+        res.iterations = m + 1;
+        if ((rc = read_scalars(ctx))) return rc;
+        const double err = ctx->h_scal[S_ERR].x;
+        res.err = err;
+        if (ctx->h_scal[S_NAN].x != 0.0 && !(err < thr)) {
+            res.status = VIE_ERR_BREAKDOWN;
+            return ctx->set_error(VIE_ERR_BREAKDOWN, "BiCORSTAB breakdown at step " + std::to_string(m));
+        }
+        if (err < thr) {
+            if (verbose) printf("Steps: %d\n\n", m);
+            res.steps = m;
+            return VIE_OK;
+        }
+        if (verbose) printf("CG Error: %lf\n", err);
+    }
+    res.status = VIE_ERR_MAXIT;
+    return VIE_OK;
+}
+
+template <typename T>
+static int solve_cg(vie_ctx* ctx, Operator<T>& op, const cplx_t<T>* b, cplx_t<T>* x, double thr, int maxit,
+                    int verbose, int vbase, KrylovResult& res) {
+    using C = cplx_t<T>;
+    int rc = VIE_OK;
+    const long long a = ctx->a, n = 3 * a;
+    C* r = (C*)work_vec(ctx, vbase + 0, sizeof(C), &rc);
+    C* p = (C*)work_vec(ctx, vbase + 1, sizeof(C), &rc);
+    C* q = (C*)work_vec(ctx, vbase + 2, sizeof(C), &rc);
+    C* Ap = (C*)work_vec(ctx, vbase + 3, sizeof(C), &rc);
+    if (rc) return rc;
+    cudaStream_t st = ctx->stream;
+    VIE_CUDA_TRY(cudaMemsetAsync(x, 0, sizeof(C) * n, st), ctx->err);
+    // r = -b (:208-216); p = A^H b (:219-229)
+    if ((rc = lin(ctx, LinArgs<C, 1, 0>{r, 0, {{b, cs(-1, -1.0)}}, {}}))) return rc;
+    if ((rc = opmv(ctx, op, ProCopy<C>{b, a}, EpiNorm<C>{p, a}, b, true))) return rc;
+    const long long nblk = epilogue_blocks(op);
+    if ((rc = finalize<1>(ctx, nblk, FinStore1{S_T0}))) return rc;  // v3 = ||p||^2
+    {
+        DotArgs<C, 1> g{{b}, {b}, {1}};
+        if ((rc = dots(ctx, g))) return rc;
+        if ((rc = finalize<1>(ctx, kVecBlocks, FinStore1{S_BNRM2}))) return rc;  // vx
+    }
+    res.matvecs += 1;
+    for (int m = 0; m < maxit; m++) {
+        if ((rc = opmv(ctx, op, ProCopy<C>{p, a}, EpiNorm<C>{Ap, a}, p, false))) return rc;  // :253-268
+        if ((rc = finalize<1>(ctx, nblk, FinCgAlpha{}))) return rc;
+        // x += alpha p; r += alpha Ap; v4 = ||r||^2 (:273-286)
+        if ((rc = lin(ctx, LinArgs<C, 1, 0>{x, 1, {{p, cs(S_ALPHA)}}, {}}))) return rc;
+        if ((rc = lin(ctx, LinArgs<C, 1, 1>{r, 1, {{Ap, cs(S_ALPHA)}}, {{nullptr, 1}}}))) return rc;
+        if ((rc = finalize<1>(ctx, kVecBlocks, FinCgErr{}))) return rc;
+        // q = A^H r; v3 = ||q||^2; beta = v3 / v1 (:291-309)
+        if ((rc = opmv(ctx, op, ProCopy<C>{r, a}, EpiNorm<C>{q, a}, r, true))) return rc;
+        if ((rc = finalize<1>(ctx, nblk, FinCgBeta{}))) return rc;
+        // p = beta p - q (:311-320)
+        if ((rc = lin(ctx, LinArgs<C, 2, 0>{p, 0, {{p, cs(S_BETA)}, {q, cs(-1, -1.0)}}, {}}))) return rc;
+        res.matvecs += 2;
+        res.iterations = m + 1;
+        if ((rc = read_scalars(ctx))) return rc;
+        const double err = ctx->h_scal[S_ERR].x;
+        res.err = err;
+        if (ctx->h_scal[S_NAN].x != 0.0 && !(err < thr)) {
+            res.status = VIE_ERR_BREAKDOWN;
+            return ctx->set_error(VIE_ERR_BREAKDOWN, "CG breakdown at step " + std::to_string(m));
+        }
+        if (err < thr) {
+            if (verbose) printf("CG Error: %lf\nSteps: %d\n\n", err, m);
+            res.steps = m;
+            return VIE_OK;
+        }
+        if (verbose) printf("CG Error: %lf\n", err);
+    }
+    res.status = VIE_ERR_MAXIT;
+    return VIE_OK;
+}
+
+template <typename T>
+static int solve_bicg(vie_ctx* ctx, Operator<T>& op, const cplx_t<T>* b, cplx_t<T>* x, double thr, int maxit,
+                      int verbose, int vbase, KrylovResult& res) {
+    using C = cplx_t<T>;
+    int rc = VIE_OK;
+    const long long a = ctx->a, n = 3 * a;
+    C* r = (C*)work_vec(ctx, vbase + 0, sizeof(C), &rc);
+    C* p = (C*)work_vec(ctx, vbase + 1, sizeof(C), &rc);
+    C* Ap = (C*)work_vec(ctx, vbase + 2, sizeof(C), &rc);
+    if (rc) return rc;
+    cudaStream_t st = ctx->stream;
+    VIE_CUDA_TRY(cudaMemsetAsync(x, 0, sizeof(C) * n, st), ctx->err);
+    VIE_CUDA_TRY(cudaMemcpyAsync(r, b, sizeof(C) * n, cudaMemcpyDeviceToDevice, st), ctx->err);  // :398-400
+    {
+        DotArgs<C, 1> g{{r}, {r}, {0}};
+        if ((rc = dots(ctx, g))) return rc;
+        if ((rc = finalize<1>(ctx, kVecBlocks, FinBicgInit{}))) return rc;  // v1 = r^T r (:402-406)
+    }
+    // p = r / v1 (:413-424)
+    if ((rc = lin(ctx, LinArgs<C, 1, 0>{p, 0, {{r, cs(S_T0)}}, {}}))) return rc;
+    const long long nblk = epilogue_blocks(op);
+    for (int m = 0; m < maxit; m++) {
+        if ((rc = opmv(ctx, op, ProCopy<C>{p, a}, EpiDotU<C>{Ap, p, a}, p, false))) return rc;  // :437-453
+        if ((rc = finalize<1>(ctx, nblk, FinBicgAlpha{}))) return rc;
+        // x += alpha p; r -= alpha Ap; v2 = r^T r (:463-479)
+        if ((rc = lin(ctx, LinArgs<C, 1, 0>{x, 1, {{p, cs(S_ALPHA)}}, {}}))) return rc;
+        if ((rc = lin(ctx, LinArgs<C, 1, 1>{r, 1, {{Ap, cs(S_ALPHA, -1.0)}}, {{nullptr, 0}}}))) return rc;
+        if ((rc = finalize<1>(ctx, kVecBlocks, FinBicgBeta{}))) return rc;
+        // p += beta r (:489-491)
+        if ((rc = lin(ctx, LinArgs<C, 1, 0>{p, 1, {{r, cs(S_BETA)}}, {}}))) return rc;
+        res.matvecs += 1;
+        res.iterations = m + 1;
+        if ((rc = read_scalars(ctx))) return rc;
+        const double err = ctx->h_scal[S_ERR].x;
+        res.err = err;
+        if (ctx->h_scal[S_NAN].x != 0.0 && !(err < thr)) {
+            res.status = VIE_ERR_BREAKDOWN;
+            return ctx->set_error(VIE_ERR_BREAKDOWN, "BiCG breakdown at step " + std::to_string(m));
+        }
+        if (err < thr) {
+            if (verbose) printf("CG Error: %lf\nSteps: %d\n\n", err, m);
+            res.steps = m;
+            return VIE_OK;
+        }
+        if (verbose) printf("CG Error: %lf\n", err);
+    }
+    res.status = VIE_ERR_MAXIT;
+    return VIE_OK;
+}
+
+template <typename T>
+static int run_solver(vie_ctx* ctx, Operator<T>& op, int solver, const cplx_t<T>* b, cplx_t<T>* x, double thr,
+                      int maxit, int verbose, int vbase, KrylovResult& res) {
+    VIE_CUDA_TRY(cudaMemsetAsync(ctx->d_scal, 0, sizeof(double2) * S_COUNT, ctx->stream), ctx->err);
+    switch (solver) {
+        case VIE_SOLVER_BICGSTAB: return solve_bicgstab<T>(ctx, op, b, x, thr, maxit, verbose, vbase, res);
+        case VIE_SOLVER_CORS: return solve_cors<T>(ctx, op, b, x, thr, maxit, verbose, vbase, res);
+        case VIE_SOLVER_CG: return solve_cg<T>(ctx, op, b, x, thr, maxit, verbose, vbase, res);
+        case VIE_SOLVER_BICG: return solve_bicg<T>(ctx, op, b, x, thr, maxit, verbose, vbase, res);
+        case VIE_SOLVER_BICORSTAB: return solve_bicorstab<T>(ctx, op, b, x, thr, maxit, verbose, vbase, res);
+        default: return ctx->set_error(VIE_ERR_ARG, "unknown solver " + std::to_string(solver));
+    }
+}
+
+// ||b - A x|| / ||b|| in FP64; r64 and the scalar slots S_T5 (||r||^2), S_BNRM2 are overwritten
+static int true_residual(vie_ctx* ctx, const double2* b, const double2* x, double2* r, double* relres,
+                         double2* bn2_slot_value) {
+    int rc;
+    const long long a = ctx->a;
+    if ((rc = opmv(ctx, ctx->op64, ProCopy<double2>{x, a}, EpiResidual<double2>{r, b, a}, x, false))) return rc;
+    if ((rc = finalize<1>(ctx, epilogue_blocks(ctx->op64), FinNorm{S_T5}))) return rc;
+    if ((rc = read_scalars(ctx))) return rc;
+    *relres = std::sqrt(ctx->h_scal[S_T5].x / bn2_slot_value->x);
+    return VIE_OK;
+}
+
+int solve_driver(vie_ctx* ctx, const vie_solve_params* prm, vie_solve_info* info) {
+    int rc = ensure_scalars(ctx);
+    if (rc) return rc;
+    const long long a = ctx->a, n = 3 * a;
+    const int maxit = prm->max_iter > 0 ? prm->max_iter : (int)std::min<long long>(a, 2000000000LL);
+    cudaStream_t st = ctx->stream;
+    cudaEvent_t e0, e1;
+    VIE_CUDA_TRY(cudaEventCreate(&e0), ctx->err);
+    VIE_CUDA_TRY(cudaEventCreate(&e1), ctx->err);
+    VIE_CUDA_TRY(cudaEventRecord(e0, st), ctx->err);
+    vie_solve_info out{};
+    out.steps = -1;
+    // masked right-hand side b (FP64) in work slot 20
+    double2* b64 = (double2*)work_vec(ctx, 20, sizeof(double2), &rc);
+    if (rc) return rc;
+    k_mask_rhs<double2><<<kVecBlocks, 256, 0, st>>>(ctx->d_rhs, ctx->d_flags, b64, a, 1.0);
+    VIE_CUDA_TRY(cudaGetLastError(), ctx->err);
+    // ||b||^2
+    {
+        DotArgs<double2, 1> g{{b64}, {b64}, {1}};
+        if ((rc = dots(ctx, g))) return rc;
+        if ((rc = finalize<1>(ctx, kVecBlocks, FinNorm{S_BNRM2}))) return rc;
+        if ((rc = read_scalars(ctx))) return rc;
+    }
+    double2 bn2 = ctx->h_scal[S_BNRM2];
+    if (!(bn2.x > 0.0)) return ctx->set_error(VIE_ERR_ARG, "right-hand side is zero on every flagged edge");
+    int status = VIE_OK;
+    if (prm->precision == VIE_PREC_FP64) {
+        KrylovResult res;
+        rc = run_solver<double>(ctx, ctx->op64, prm->solver, b64, ctx->d_x, prm->tol, maxit, prm->verbose, 0, res);
+        if (rc) return rc;
+        status = res.status;
+        out.steps = res.steps;
+        out.iterations = res.iterations;
+        out.matvecs_fp64 = res.matvecs;
+        out.relres = res.err;
+    } else if (prm->precision == VIE_PREC_MIXED) {
+        // FP32 inner Krylov inside FP64 defect correction:
+        //   r = b - A x (FP64);  solve A d = r / ||r|| in FP32;  x += ||r|| d (FP64)
+        const double inner_tol = prm->inner_tol > 0 ? prm->inner_tol : 1e-4;
+        const int max_outer = prm->max_outer > 0 ? prm->max_outer : 30;
+        double2* r64 = (double2*)work_vec(ctx, 21, sizeof(double2), &rc);
+        float2* b32 = (float2*)work_vec(ctx, 22, sizeof(float2), &rc);
+        float2* d32 = (float2*)work_vec(ctx, 23, sizeof(float2), &rc);
+        if (rc) return rc;
+        VIE_CUDA_TRY(cudaMemsetAsync(ctx->d_x, 0, sizeof(double2) * n, st), ctx->err);
+        VIE_CUDA_TRY(cudaMemcpyAsync(r64, b64, sizeof(double2) * n, cudaMemcpyDeviceToDevice, st), ctx->err);
+        double relres = 1.0;
+        double2 rr = bn2;
+        int outer = 0;
+        while (true) {
+            relres = std::sqrt(rr.x / bn2.x);
+            if (relres < prm->tol) break;
+            if (outer >= max_outer) { status = VIE_ERR_MAXIT; break; }
+            if (out.iterations >= maxit) { status = VIE_ERR_MAXIT; break; }
+            // r32 = r64 / ||r||
+            {
+                // put ||r||^2 in S_T5 for the scaling kernels
+                VIE_CUDA_TRY(cudaMemcpyAsync(ctx->d_scal + S_T5, &rr, sizeof(double2), cudaMemcpyHostToDevice, st),
+                             ctx->err);
+                VIE_CUDA_TRY(cudaStreamSynchronize(st), ctx->err);
+                k_scale_to<float2><<<kVecBlocks, 256, 0, st>>>(b32, r64, n, ctx->d_scal, S_T5);
+                VIE_CUDA_TRY(cudaGetLastError(), ctx->err);
+            }
+            KrylovResult res;
+            const double itol = std::max(inner_tol, 0.5 * prm->tol / relres);
+            rc = run_solver<float>(ctx, ctx->op32, prm->solver, b32, d32, itol, maxit - out.iterations, prm->verbose,
+                                   8, res);
+            if (rc && rc != VIE_ERR_BREAKDOWN) return rc;
+            out.iterations += res.iterations;
+            out.matvecs_fp32 += res.matvecs;
+            // x += ||r|| d  (scale from S_T5 = ||r||^2 saved before the inner solve overwrote slots)
+            VIE_CUDA_TRY(cudaMemcpyAsync(ctx->d_scal + S_T5, &rr, sizeof(double2), cudaMemcpyHostToDevice, st),
+                         ctx->err);
+            k_accum_d<float2><<<kVecBlocks, 256, 0, st>>>(ctx->d_x, d32, n, ctx->d_scal, S_T5, 1);
+            VIE_CUDA_TRY(cudaGetLastError(), ctx->err);
+            // r = b - A x in FP64
+            double rel;
+            if ((rc = true_residual(ctx, b64, ctx->d_x, r64, &rel, &bn2))) return rc;
+            out.matvecs_fp64 += 1;
+            rr = ctx->h_scal[S_T5];
+            outer++;
+            if (res.status == VIE_ERR_BREAKDOWN && rel >= relres) {
+                status = VIE_ERR_BREAKDOWN;
+                relres = rel;
+                break;
+            }
+        }
+        ctx->err.code = VIE_OK;
+        out.outer = outer;
+        out.relres = std::sqrt(rr.x / bn2.x);
+        out.steps = out.iterations > 0 ? out.iterations - 1 : 0;
+    } else {
+        return ctx->set_error(VIE_ERR_ARG, "unknown precision mode");
+    }
+    VIE_CUDA_TRY(cudaEventRecord(e1, st), ctx->err);
+    VIE_CUDA_TRY(cudaEventSynchronize(e1), ctx->err);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    out.seconds = ms * 1e-3;
+    // true residual in FP64 (not timed)
+    {
+        double2* r64 = (double2*)work_vec(ctx, 21, sizeof(double2), &rc);
+        if (rc) return rc;
+        double rel;
+        if ((rc = true_residual(ctx, b64, ctx->d_x, r64, &rel, &bn2))) return rc;
+        out.true_relres = rel;
+    }
+    ctx->have_x = true;
+    if (info) *info = out;
+    if (status == VIE_ERR_MAXIT)
+        return ctx->set_error(VIE_ERR_MAXIT, "iteration cap reached before the tolerance");
+    if (status == VIE_ERR_BREAKDOWN)
+        return ctx->set_error(VIE_ERR_BREAKDOWN, "Krylov breakdown before the tolerance");
+    return VIE_OK;
+}
+
+}  // namespace vie
