@@ -1,0 +1,411 @@
+#!/usr/bin/env python
+"""Benchmark of the VIE solve on B200 (one JSON line on rank 0).
+
+Workload (default ``c3``): 256^3 organic solar cell (PEDOT 40 nm, P3HT:PCBM
+120 nm, 16 Ag spheres r = 20 nm seeded in the active layer), 1 nm voxels,
+padded 512^3, x-polarised plane wave at 550 nm, BiCGSTAB to relative
+residual 1e-8 from x0 = 0.  Synthetic geometry from vie_fft_b200.geometry.
+
+One step = one full solve on inputs resident in HBM: FP32-complex inner
+BiCGSTAB inside FP64 defect correction (``value``, solves/s).  The all-FP64
+solve of the same system is timed after it for the speed-up, and the
+operator application (the hot op) is timed on its own for the roofline.
+
+``e2e`` times the same solve through the C ABI with host buffers: every step
+copies the incident field from pinned host memory to the device and the
+solution back (both inside the timed region).
+
+``--impl reference`` times the reference's own CPU code (oracle/_ref: the
+reference vie_fft compiled against the MKL shim; the C restatement when the
+reference build is absent) on a bounded sample of the same workload: one
+L_DC_Dq block (two 512^3 FFTs, the spectral multiply, the crop) per process,
+one process per usable host core, scaled to solves/s with the operator's nine
+blocks per application and the FP64 iteration count of this workload.
+
+Multi-GPU: replicas only (instances are independent, like the reference's
+per-wavelength process farm); value = total solves / max time over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "solves/s & matvec ms to rel-res 1e-8: mixed vs FP64 on 1 B200; % HBM peak"
+TOL = 1e-8
+# BiCGSTAB iterations of the FP64 solve of this workload to 1e-8 on the GPU
+# (measured; used only to scale the CPU sample to solves/s)
+FP64_ITERS = {"c3": 525, "c2": 21, "c1": 36}
+
+
+def workload(name):
+    from vie_fft_b200 import geometry as G
+    if name == "c3":
+        return G.solar_cell(), "256^3 organic solar cell (PEDOT/P3HT:PCBM, 16 Ag spheres r=20nm), 1 nm voxels, " \
+                               "padded 512^3, x-pol 550 nm, BiCGSTAB to rel-res 1e-8"
+    if name == "c2":
+        return G.sphere_cluster(), "128^3 cluster of 40 Au spheres (r 5-15 nm, seed 2) in eps_b=1.77, 1 nm voxels, " \
+                                   "padded 256^3, x-pol 500 nm, BiCGSTAB to rel-res 1e-8"
+    if name == "c1":
+        return G.single_sphere(), "32^3 Ag sphere r=18 nm, 1.25 nm voxels, padded 64^3, x-pol 400 nm"
+    raise SystemExit(f"unknown workload {name}")
+
+
+def bytes_per_matvec(shape, e):
+    """Algorithmic HBM bytes of one operator application (five pruned passes):
+    e*(3*(3a + 4b + 4c) + g) + a, a = NxNyNz, b = NxNy*2Nz, c = Nx*2Ny*2Nz,
+    g = the (Nx+1)(Ny+1)(Nz+1) Green octant, + a bytes of edge flags."""
+    nx, ny, nz = shape
+    a = nx * ny * nz
+    b = nx * ny * 2 * nz
+    c = nx * 2 * ny * 2 * nz
+    g = (nx + 1) * (ny + 1) * (nz + 1)
+    return e * (3 * (3 * a + 4 * b + 4 * c) + g) + a
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    def __init__(self, gpu_index):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={gpu_index}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        self.p.wait()
+        self.f.seek(0)
+        rows = [l.strip().split(", ") for l in self.f.read().splitlines() if l.strip()]
+        os.unlink(self.f.name)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                smax = float(r[2])
+                for nm_, v in zip(names, r[5:9]):
+                    if v.strip() == "Active":
+                        reasons.add(nm_)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# reference / CPU baseline
+# ---------------------------------------------------------------------------
+def _block_worker(args):
+    shape, d, k0, use_ref = args
+    from oracle import oracle as O
+    return O.time_block(O.Grid(*shape, *d, k0), use_reference=use_ref)
+
+
+def cpu_block_sample(w, procs, use_ref=True):
+    """Time one L_DC_Dq block of workload w in `procs` concurrent processes."""
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(procs) as pool:
+        res = pool.map(_block_worker, [(w.shape, w.d, w.k0, use_ref)] * procs)
+    wall = time.perf_counter() - t0
+    return res, wall
+
+
+def usable_cores(w):
+    n = os.cpu_count() or 1
+    try:
+        import psutil
+        mem = psutil.virtual_memory().available
+    except Exception:
+        mem = 8 << 30
+    per = 16 * 8 * w.a * 2 + 16 * w.a * 4  # Green + padded array + vectors of one block
+    return max(1, min(n, int(mem * 0.6 // per), 64))
+
+
+def cpu_solves_per_s(block_seconds, iters):
+    # one BiCGSTAB iteration = 2 operator applications = 2 x 9 blocks
+    return 1.0 / (block_seconds * 9 * 2 * iters)
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    w, desc = workload(args.workload)
+    from oracle import oracle as O
+    use_ref = O.ref_available()
+    kind = "reference" if use_ref else "port"
+    iters = args.fp64_iters or FP64_ITERS.get(args.workload) or 0
+    procs = usable_cores(w)
+    # warm-up: the same block on a 64^3 grid (pages in code and allocator)
+    for _ in range(max(args.warmup, 1)):
+        _block_worker(((64, 64, 64), w.d, w.k0, use_ref))
+    times = []
+    for _ in range(args.steps):
+        res, wall = cpu_block_sample(w, procs, use_ref)
+        per = max(r["seconds"] for r in res)
+        times.append(per)
+    block = statistics.median(times)
+    # aggregate over the processes that ran concurrently
+    value = procs * cpu_solves_per_s(block, iters) if iters else None
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": block * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+            "config": {"workload": desc, "grid": list(w.shape), "parallelism": "processes"},
+            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": procs, "kind": kind,
+                             "sample": f"one L_DC_Dq block (two {2*w.shape[0]}^3 FFTs + multiply + crop) per "
+                                       f"process, {procs} processes; solves/s = procs / (block_s * 9 blocks * "
+                                       f"2 matvecs * {iters} FP64 iterations)",
+                             "block_seconds": block},
+            "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def run_gpu(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+
+    import vie_fft_b200 as V
+    from vie_fft_b200 import post
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    w, desc = workload(args.workload)
+    if world > 1:
+        # replicas: each rank solves its own wavelength of the same geometry
+        from vie_fft_b200 import geometry as G
+        w.k0 = G.k0_of(w.meta["wavelength_nm"] + 5.0 * rank)
+    c = V.Context(*w.shape, *w.d, w.k0, device=local_rank)
+    c.set_flags(w.flags)
+    if w.eps_voxel is not None:
+        c.set_eps(w.eps_voxel)
+    else:
+        c.set_material(w.material, w.eps_table)
+    t0 = time.perf_counter()
+    c.green()
+    green_s = time.perf_counter() - t0
+    c.incident(w.theta, w.phi, w.psi, copy=False)
+    stream = torch.cuda.ExternalStream(c.stream_ptr())
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    def solve(precision, true_residual=False, out=None):
+        r = c.solve("bicgstab", tol=TOL, precision=precision, copy=out is not None, out=out,
+                    true_residual=true_residual)
+        return r
+
+    # ---- warm-up
+    for _ in range(args.warmup):
+        last = solve(V.PREC_MIXED)
+    # ---- timed region: K mixed solves
+    barrier()
+    sampler = ClockSampler(local_rank) if rank == 0 else None
+    launches0 = V.launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    infos = []
+    for _ in range(args.steps):
+        infos.append(solve(V.PREC_MIXED).info)
+    ev1.record(stream)
+    ev1.synchronize()
+    barrier()
+    launches = V.launch_count() - launches0
+    clocks = sampler.stop() if sampler else None
+    ms = ev0.elapsed_time(ev1) / args.steps
+    t_all = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        dist.all_reduce(t_all, op=dist.ReduceOp.MAX)
+    ms_max = float(t_all.item())
+    value = world * 1e3 / ms_max
+    x_mixed = c.solution()
+
+    # ---- FP64 reference solve of the same system (speed-up and accuracy)
+    solve(V.PREC_FP64)
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    n64 = max(1, min(2, args.steps))
+    for _ in range(n64):
+        r64 = solve(V.PREC_FP64)
+    e1.record(stream)
+    e1.synchronize()
+    ms64 = e0.elapsed_time(e1) / n64
+    x64 = c.solution()
+    rel64 = {"true_relres": c.residual()}
+
+    # ---- operator roofline (the hot op of each precision), inputs > L2
+    def time_matvec(dtype, prec, reps=10):
+        x = torch.randn((3,) + w.shape, dtype=dtype, device="cuda")
+        y = torch.zeros_like(x)
+        torch.cuda.synchronize()
+        for _ in range(3):
+            c.matvec_dev(x.data_ptr(), y.data_ptr(), precision=prec)
+        c.sync()
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        for _ in range(reps):
+            c.matvec_dev(x.data_ptr(), y.data_ptr(), precision=prec)
+        a1.record(stream)
+        a1.synchronize()
+        del x, y
+        return a0.elapsed_time(a1) / reps
+
+    mv32 = time_matvec(torch.complex64, V.PREC_MIXED)
+    mv64 = time_matvec(torch.complex128, V.PREC_FP64)
+    peak, peak_kind = measured_peaks()
+    B32, B64 = bytes_per_matvec(w.shape, 8), bytes_per_matvec(w.shape, 16)
+    ach32 = B32 / (mv32 * 1e-3) / 1e9
+    ach64 = B64 / (mv64 * 1e-3) / 1e9
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "matvec_dram_bytes.json")
+    if os.path.exists(tf):
+        with open(tf) as f:
+            tj = json.load(f)
+        traffic = tj.get(args.workload, {}).get("fp32")
+
+    # ---- end to end through the C ABI with pinned host buffers
+    e2e = None
+    if args.e2e_steps > 0:
+        h_rhs = torch.empty((3,) + w.shape, dtype=torch.complex128, pin_memory=True)
+        h_x = torch.empty((3,) + w.shape, dtype=torch.complex128, pin_memory=True)
+        e_host = c.incident(w.theta, w.phi, w.psi, copy=True)
+        h_rhs.numpy()[...] = e_host
+        xn = h_x.numpy()
+        barrier()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        tw0 = time.perf_counter()
+        f0.record(stream)
+        for _ in range(args.e2e_steps):
+            c.set_rhs(h_rhs.numpy())
+            c.solve("bicgstab", tol=TOL, precision=V.PREC_MIXED, out=xn, true_residual=False)
+        f1.record(stream)
+        f1.synchronize()
+        wall = (time.perf_counter() - tw0) / args.e2e_steps
+        ms_e2e = f0.elapsed_time(f1) / args.e2e_steps
+        te = torch.tensor([ms_e2e], dtype=torch.float64, device="cuda")
+        if dist is not None:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        e2e = {"value": world * 1e3 / float(te.item()), "unit": "solves/s",
+               "h2d_bytes_per_step": int(h_rhs.numel() * 16), "d2h_bytes_per_step": int(h_x.numel() * 16),
+               "wall_ms_per_step": wall * 1e3}
+
+    if rank != 0:
+        return
+    # ---- accuracy of the mixed solve against FP64
+    cs_mixed = post.cross_sections(w, x_mixed)
+    cs_64 = post.cross_sections(w, x64)
+    xerr = {k: abs(cs_mixed[k] - cs_64[k]) / max(abs(cs_64[k]), 1e-300) for k in cs_64}
+    field_rel = float(np.linalg.norm(x_mixed - x64) / np.linalg.norm(x64))
+
+    # ---- CPU baseline (bounded sample), rank 0 at N = 1 only
+    cpu = None
+    if world == 1 and not args.no_cpu:
+        from oracle import oracle as O
+        use_ref = O.ref_available()
+        res, wall = cpu_block_sample(w, 1, use_ref)
+        blk = res[0]["seconds"]
+        iters64 = r64.info["iterations"]
+        cpu = {"value": cpu_solves_per_s(blk, iters64), "unit": "solves/s", "cores": 1, "kind": res[0]["kind"],
+               "sample": f"one L_DC_Dq block at {w.shape} ({2*w.shape[0]}^3 padded FFT pair, {blk:.1f} s), "
+                         f"scaled by 9 blocks x 2 matvecs x {iters64} FP64 BiCGSTAB iterations",
+               "block_seconds": blk}
+
+    info = infos[-1]
+    line = {
+        "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "c64 inner + c128 refine", "data": "synthetic",
+        "config": {"workload": desc, "grid": list(w.shape), "padded": [2 * s for s in w.shape],
+                   "solver": "bicgstab", "tol": TOL, "precision": "mixed (FP32 inner Krylov, FP64 defect correction)",
+                   "l2": "inputs larger than L2 (FP32 vectors 403 MB, FP64 805 MB each)",
+                   "parallelism": "replicas" if world > 1 else "single"},
+        "roofline": {"bound": "hbm", "achieved": ach32, "peak": peak, "unit": "GB/s", "frac": ach32 / peak,
+                     "traffic": traffic, "kernel": "FP32 operator application (5 pruned FFT passes)",
+                     "peak_source": peak_kind, "algorithmic_bytes": B32},
+        "e2e": e2e,
+        "gpu_launches": launches,
+        "clocks": clocks,
+        "cpu_baseline": cpu,
+        "fp64": {"solves_per_s": 1e3 / ms64, "ms_per_solve": ms64, "iterations": r64.info["iterations"],
+                 "true_relres": rel64["true_relres"]},
+        "speedup_mixed_vs_fp64": ms64 / ms_max,
+        "mixed": {"iterations": info["iterations"], "outer": info["outer"], "matvecs_fp32": info["matvecs_fp32"],
+                  "matvecs_fp64": info["matvecs_fp64"], "true_relres": info["true_relres"]},
+        "matvec_ms": {"fp32": mv32, "fp64": mv64},
+        "matvec_hbm_frac": {"fp32": ach32 / peak, "fp64": ach64 / peak},
+        "xsec_rel_err_mixed_vs_fp64": xerr, "field_rel_diff_mixed_vs_fp64": field_rel,
+        "green_setup_s": green_s,
+    }
+    print(json.dumps(line), flush=True)
+    c.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="vie", choices=["vie", "reference"])
+    ap.add_argument("--workload", default="c3", choices=["c1", "c2", "c3"])
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--fp64-iters", type=int, default=0)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    try:
+        run_gpu(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

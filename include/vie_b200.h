@@ -113,6 +113,8 @@ typedef struct {
     double inner_tol;   /* mixed: inner reduction per refinement step (<= 0: 1e-4) */
     int max_outer;      /* mixed: refinement cap (<= 0: 30) */
     int verbose;        /* print "CG Error" per iteration like the reference */
+    int true_residual;  /* FP64 solves: evaluate ||b - A x|| / ||b|| at exit (one more
+                           operator application); mixed solves always report it */
 } vie_solve_params;
 
 typedef struct {
@@ -122,7 +124,7 @@ typedef struct {
     int matvecs_fp64;   /* operator applications in FP64 */
     int matvecs_fp32;   /* operator applications in FP32 */
     double relres;      /* the solver's own residual estimate at exit */
-    double true_relres; /* ||b - A x|| / ||b|| evaluated in FP64 at exit */
+    double true_relres; /* ||b - A x|| / ||b|| in FP64 at exit (-1 when not evaluated) */
     double seconds;     /* device time of the solve */
 } vie_solve_info;
 
@@ -130,6 +132,9 @@ typedef struct {
    FFT_Program (CG_Iteration.h:1365-1388) and the driver it dispatches to.
    x (3a complex) may be NULL; the solution also stays on the device. */
 VIE_API int vie_solve(vie_ctx* ctx, const vie_solve_params* p, double* x, vie_solve_info* info);
+/* ||b - A x|| / ||b|| of the last solution for the current right-hand side,
+   evaluated in FP64 (one operator application). */
+VIE_API int vie_residual(vie_ctx* ctx, double* relres);
 /* Copy the last solution (Current_X/Y/Z) to the host, 3a complex. */
 VIE_API int vie_get_solution(vie_ctx* ctx, double* x);
 /* Device pointer of the last solution (3a double2), valid until the next solve. */
@@ -144,6 +149,9 @@ VIE_API int vie_sync(vie_ctx* ctx);
 /* The context's CUDA stream (a cudaStream_t), for callers that order their
    own work or record timing events on it. */
 VIE_API int vie_stream(vie_ctx* ctx, void** stream);
+
+/* Number of CUDA kernels this library has launched in this process. */
+VIE_API long long vie_launch_count(void);
 
 /* Library version string. */
 VIE_API const char* vie_version(void);

@@ -91,6 +91,7 @@ def lib():
             L.vo_farfield1.argtypes = [g, _dp, ctypes.c_double, ctypes.c_double, ctypes.c_double]
             L.vo_farfield1.restype = ctypes.c_double
             L.vo_absorption.argtypes = [g, _dp, _dp, _up, ctypes.c_int, ctypes.c_int, _dp, _dp, _dp]
+            L.vo_block.argtypes = [g, _dp, _dp, _dp]
             _oracle = L
     return _oracle
 
@@ -296,3 +297,27 @@ def fft3d(x, sign=-1) -> np.ndarray:
     if L.vo_fft3d(_p(y), n0, n1, n2, int(sign)):
         raise RuntimeError("vo_fft3d failed")
     return y
+
+
+def time_block(g: Grid, use_reference: bool = True) -> dict:
+    """Seconds of one L_DC_Dq block (fft.h:41-127) at grid g: two (2N)^3 FFTs,
+    the spectral multiply and the crop, on the reference build when present,
+    else on the restatement.  The unit of the CPU baseline."""
+    import time
+    n = g.shape
+    pad = np.zeros((2 * n[0], 2 * n[1], 2 * n[2]), np.complex128)
+    pad[: n[0] - 1, : n[1], : n[2]] = 1.0 + 0.5j
+    fld = np.zeros(n, np.complex128)
+    if use_reference and ref_available():
+        R = Reference(g, np.array([1.1, 2.0, 2.0, 2.0]))
+        R.L.ref_green(None)
+        t = time.perf_counter()
+        R.L.ref_time_block(_p(pad), _p(fld))
+        dt = time.perf_counter() - t
+        R.release()
+        return {"seconds": dt, "kind": "reference"}
+    G = green(g)
+    t = time.perf_counter()
+    lib().vo_block(ctypes.byref(g.c()), _p(G), _p(pad), _p(fld))
+    return {"seconds": time.perf_counter() - t, "kind": "port"}
+

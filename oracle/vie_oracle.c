@@ -594,3 +594,18 @@ int vo_absorption(const vo_grid* g, const double* xin, const double* eps_in,
     if (active_volume) *active_volume = av;
     return 0;
 }
+
+/* One self-term block exactly as L_DC_Dq (fft.h:41-127) does it on an already
+   expanded (2N)^3 current: forward FFT, spectral multiply, backward FFT,
+   field += crop.  Used to time the CPU baseline per block. */
+int vo_block(const vo_grid* g, const double* green, double* padded, double* field) {
+    op_ctx o;
+    if (op_init(&o, g, green, NULL, NULL)) { op_free(&o); return 1; }
+    free(o.tmp);
+    o.tmp = (cx*)padded;
+    int rc = fft_block(&o, (cx*)field, 0, 0, 0);
+    o.tmp = NULL;
+    op_free(&o);
+    return rc;
+}
+

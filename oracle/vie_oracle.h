@@ -64,6 +64,10 @@ int vo_absorption(const vo_grid* g, const double* x, const double* eps,
                   const unsigned char* material, int metal_label, int active_label,
                   double* metal_abs, double* active_abs, double* active_volume);
 
+/* One L_DC_Dq block (fft.h:41-127) on an expanded (2nx,2ny,2nz) current
+   (modified in place) accumulating into field (a complex); for timing. */
+int vo_block(const vo_grid* g, const double* green, double* padded, double* field);
+
 #ifdef __cplusplus
 }
 #endif

@@ -54,7 +54,7 @@ class VieGrid(ctypes.Structure):
 class VieSolveParams(ctypes.Structure):
     _fields_ = [("solver", ctypes.c_int), ("precision", ctypes.c_int), ("tol", ctypes.c_double),
                 ("max_iter", ctypes.c_int), ("inner_tol", ctypes.c_double), ("max_outer", ctypes.c_int),
-                ("verbose", ctypes.c_int)]
+                ("verbose", ctypes.c_int), ("true_residual", ctypes.c_int)]
 
 
 class VieSolveInfo(ctypes.Structure):
@@ -87,6 +87,7 @@ def lib():
         L.vie_status_string.argtypes = [ctypes.c_int]
         L.vie_status_string.restype = ctypes.c_char_p
         L.vie_version.restype = ctypes.c_char_p
+        L.vie_launch_count.restype = ctypes.c_longlong
         L.vie_set_material.argtypes = [_vp, _up, _dp, _dp, ctypes.c_int]
         L.vie_set_eps.argtypes = [_vp, _dp]
         L.vie_set_flags.argtypes = [_vp, _up, _up, _up]
@@ -98,6 +99,7 @@ def lib():
         L.vie_matvec_dev.argtypes = [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int]
         L.vie_solve.argtypes = [_vp, P(VieSolveParams), _dp, P(VieSolveInfo)]
         L.vie_get_solution.argtypes = [_vp, _dp]
+        L.vie_residual.argtypes = [_vp, _dp]
         L.vie_solution_device.argtypes = [_vp, P(_vp)]
         L.vie_rhs_device.argtypes = [_vp, P(_vp)]
         L.vie_sync.argtypes = [_vp]
@@ -213,14 +215,21 @@ class Context:
         self._check(self._L.vie_matvec_dev(self._h, _vp(x_ptr), _vp(y_ptr), int(bool(conj)), int(precision)))
 
     def solve(self, solver="bicgstab", tol=1e-3, precision=PREC_FP64, max_iter=0, inner_tol=0.0, max_outer=0,
-              verbose=False, copy=True, allow_maxit=False):
+              verbose=False, copy=True, allow_maxit=False, true_residual=True, out=None):
         prm = VieSolveParams(SOLVERS[solver] if isinstance(solver, str) else int(solver), int(precision),
-                             float(tol), int(max_iter), float(inner_tol), int(max_outer), int(bool(verbose)))
+                             float(tol), int(max_iter), float(inner_tol), int(max_outer), int(bool(verbose)),
+                             int(bool(true_residual)))
         info = VieSolveInfo()
-        x = np.zeros((3,) + self.shape, np.complex128) if copy else None
+        x = out if out is not None else (np.zeros((3,) + self.shape, np.complex128) if copy else None)
         rc = self._L.vie_solve(self._h, ctypes.byref(prm), _p(x) if copy else None, ctypes.byref(info))
         self._check(rc, allow=(VIE_ERR_MAXIT,) if allow_maxit else ())
         return SolveResult(x, info.as_dict(), rc)
+
+    def residual(self) -> float:
+        """||b - A x|| / ||b|| of the last solution, in FP64."""
+        v = ctypes.c_double(0)
+        self._check(self._L.vie_residual(self._h, ctypes.byref(v)))
+        return v.value
 
     def solution(self):
         x = np.zeros((3,) + self.shape, np.complex128)
@@ -245,6 +254,11 @@ class Context:
 
     def sync(self):
         self._check(self._L.vie_sync(self._h))
+
+
+def launch_count() -> int:
+    """Kernels launched by the library in this process so far."""
+    return int(lib().vie_launch_count())
 
 
 def version() -> str:

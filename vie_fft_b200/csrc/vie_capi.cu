@@ -13,9 +13,12 @@ int green_compute(vie_ctx* ctx);
 int green_expand(vie_ctx* ctx, double2* d_out);
 int incident_compute(vie_ctx* ctx, double theta, double phi, double psi, double2* d_e);
 int solve_driver(vie_ctx* ctx, const vie_solve_params* prm, vie_solve_info* info);
+int residual_driver(vie_ctx* ctx, double* relres);
 }  // namespace vie
 
 using namespace vie;
+
+std::atomic<long long> vie::g_launches{0};
 
 namespace {
 
@@ -66,6 +69,8 @@ int upload_contrast(vie_ctx* ctx) {
 }  // namespace
 
 extern "C" {
+
+long long vie_launch_count(void) { return g_launches.load(); }
 
 const char* vie_version(void) { return "vie_b200 0.1 (sm_100a)"; }
 
@@ -304,6 +309,15 @@ int vie_solve(vie_ctx* ctx, const vie_solve_params* p, double* x, vie_solve_info
         if (e != cudaSuccess && !rc) rc = ctx->set_error(VIE_ERR_CUDA, cudaGetErrorString(e));
     }
     return rc;
+}
+
+int vie_residual(vie_ctx* ctx, double* relres) {
+    if (check_ctx(ctx) || !relres) return VIE_ERR_ARG;
+    int rc = ready_for_operator(ctx);
+    if (rc) return rc;
+    if (!ctx->have_rhs || !ctx->have_x) return ctx->set_error(VIE_ERR_STATE, "no solution yet (vie_solve)");
+    cudaSetDevice(ctx->device);
+    return residual_driver(ctx, relres);
 }
 
 int vie_get_solution(vie_ctx* ctx, double* x) {

@@ -167,6 +167,7 @@ int green_compute(vie_ctx* ctx) {
     const double si = p * std::cos(p) - std::sin(p);          // Im((1+ip)(cos p - i sin p))
     const double2 self = make_double2(sr / den * dV, si / den * dV);
     k_green_spatial<<<1184, 256, 0, ctx->stream>>>(ctx->d_green, nx, ny, nz, dx, dy, dz, k0, amp, self);
+    count_launch();
     VIE_CUDA_TRY(cudaGetLastError(), err);
     const int n3[3] = {nx, ny, nz};
     const long long E[3] = {nx + 1, ny + 1, nz + 1};
@@ -194,6 +195,7 @@ int green_compute(vie_ctx* ctx) {
         }
         VIE_CUDA_TRY(cudaFuncSetAttribute(k_dct1_axis, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), err);
         k_dct1_axis<<<148 * 8, 256, smem, ctx->stream>>>(ctx->d_green, (int)len, inner, outer, d_cos + ax * 2 * maxN);
+        count_launch();
         VIE_CUDA_TRY(cudaGetLastError(), err);
     }
     VIE_CUDA_TRY(cudaStreamSynchronize(ctx->stream), err);
@@ -203,6 +205,7 @@ int green_compute(vie_ctx* ctx) {
 
 int green_expand(vie_ctx* ctx, double2* d_out) {
     k_green_expand<<<1184, 256, 0, ctx->stream>>>(ctx->d_green, d_out, ctx->nx, ctx->ny, ctx->nz);
+    count_launch();
     VIE_CUDA_TRY(cudaGetLastError(), ctx->err);
     return VIE_OK;
 }
@@ -217,6 +220,7 @@ int incident_compute(vie_ctx* ctx, double theta, double phi, double psi, double2
     const double pz = -std::sin(th) * std::cos(ps);                                              // :243-244
     k_incident<<<1184, 256, 0, ctx->stream>>>(d_e, ctx->nx, ctx->ny, ctx->nz, ctx->d[0], ctx->d[1], ctx->d[2], kx, ky,
                                               kz, px, py, pz, 1.0e-7);
+    count_launch();
     VIE_CUDA_TRY(cudaGetLastError(), ctx->err);
     return VIE_OK;
 }

@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 #include <string>
@@ -11,6 +12,11 @@
 #include "vie_operator.cuh"
 
 namespace vie {
+
+// Kernel launches issued by this library in this process (every <<<>>> site
+// adds to it right after the launch).
+extern std::atomic<long long> g_launches;
+inline void count_launch(long long n = 1) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 constexpr double kPI = 3.1415926535897932384626433832795;  // common.h:17
 constexpr double kZ0 = 120 * kPI;                            // common.h:18

@@ -47,34 +47,41 @@ int launch_operator(Operator<T>& op, Pro pro, Epi epi, const cplx_t<T>* xdiag, b
         auto kf = k_fwd_z<C, Pro>;
         VIE_CUDA_TRY(ensure_smem(kf, op.smem_z), err);
         kf<<<dim3(ceil_div(nrows, d.tz), 3), kThreads, op.smem_z, st>>>(d, pro);
+        count_launch();
     }
     {
         auto kf = k_fwd_y<C>;
         VIE_CUDA_TRY(ensure_smem(kf, op.smem_y), err);
         kf<<<dim3(ceil_div(Lz, d.tc), d.nx, 3), kThreads, op.smem_y, st>>>(d);
+        count_launch();
     }
     if (conj) {
         auto kf = k_x_spectral<C, true>;
         VIE_CUDA_TRY(ensure_smem(kf, op.smem_x), err);
         kf<<<dim3(ceil_div(Lz, d.tx), Ly), kThreads, op.smem_x, st>>>(d);
+        count_launch();
     } else {
         auto kf = k_x_spectral<C, false>;
         VIE_CUDA_TRY(ensure_smem(kf, op.smem_x), err);
         kf<<<dim3(ceil_div(Lz, d.tx), Ly), kThreads, op.smem_x, st>>>(d);
+        count_launch();
     }
     {
         auto kf = k_inv_y<C>;
         VIE_CUDA_TRY(ensure_smem(kf, op.smem_y), err);
         kf<<<dim3(ceil_div(Lz, d.tc), d.nx, 3), kThreads, op.smem_y, st>>>(d);
+        count_launch();
     }
     if (conj) {
         auto kf = k_inv_z<C, true, Epi>;
         VIE_CUDA_TRY(ensure_smem(kf, op.smem_z), err);
         kf<<<dim3(ceil_div(nrows, d.tz), 3), kThreads, op.smem_z, st>>>(d, xdiag, epi, partial);
+        count_launch();
     } else {
         auto kf = k_inv_z<C, false, Epi>;
         VIE_CUDA_TRY(ensure_smem(kf, op.smem_z), err);
         kf<<<dim3(ceil_div(nrows, d.tz), 3), kThreads, op.smem_z, st>>>(d, xdiag, epi, partial);
+        count_launch();
     }
     VIE_CUDA_TRY(cudaGetLastError(), err);
     return VIE_OK;

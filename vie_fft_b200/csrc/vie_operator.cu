@@ -198,6 +198,7 @@ int Operator<T>::set_green(const double2* d_oct64, double k0, cudaStream_t st, E
     const double M = 8.0 * (double)dev.nx * dev.ny * dev.nz;
     // c = i Z0 / (k0 M): the 1/M and i Z0/k0 factors of V5/V6 (fft.h:76-77, 256)
     k_scale_green<C><<<592, 256, 0, st>>>(d_oct64, d_Gs, goct, 0.0, kZ0 / (k0 * M));
+    count_launch();
     VIE_CUDA_TRY(cudaGetLastError(), err);
     return VIE_OK;
 }

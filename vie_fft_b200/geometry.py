@@ -120,13 +120,44 @@ def _sphere_label(centres, radii, inside=2):
     radii = np.asarray(radii, np.float64)
 
     def lab(x, y, z):
-        out = np.zeros(np.broadcast_shapes(np.shape(x), np.shape(y), np.shape(z)), np.uint8)
+        shp = np.broadcast_shapes(np.shape(x), np.shape(y), np.shape(z))
+        out = np.zeros(shp, np.uint8)
+        axes = _axis_vectors(x, y, z, shp)
         for (cx, cy, cz), r in zip(centres, radii):
-            # distance from the centre as Model.h:227, inside when <= radius (:229)
-            v = np.sqrt((x - cx) ** 2 + (y - cy) ** 2 + (z - cz) ** 2)
-            out = np.where(v <= r, np.uint8(inside), out)
+            if axes is not None:
+                # only the bounding box of the sphere can be inside it
+                sl = []
+                for v, c in zip(axes, (cx, cy, cz)):
+                    idx = np.nonzero(np.abs(v - c) <= r * (1 + 1e-12) + 1e-15)[0]
+                    if idx.size == 0:
+                        break
+                    sl.append(slice(int(idx[0]), int(idx[-1]) + 1))
+                if len(sl) < 3:
+                    continue
+                xs = np.asarray(x)[sl[0], :, :] if np.ndim(x) == 3 and np.shape(x)[0] > 1 else x
+                ys = np.asarray(y)[:, sl[1], :] if np.ndim(y) == 3 and np.shape(y)[1] > 1 else y
+                zs = np.asarray(z)[:, :, sl[2]] if np.ndim(z) == 3 and np.shape(z)[2] > 1 else z
+                # distance from the centre as Model.h:227, inside when <= radius (:229)
+                v = np.sqrt((xs - cx) ** 2 + (ys - cy) ** 2 + (zs - cz) ** 2)
+                sub = out[sl[0], sl[1], sl[2]]
+                out[sl[0], sl[1], sl[2]] = np.where(v <= r, np.uint8(inside), sub)
+            else:
+                v = np.sqrt((x - cx) ** 2 + (y - cy) ** 2 + (z - cz) ** 2)
+                out = np.where(v <= r, np.uint8(inside), out)
         return out
     return lab
+
+
+def _axis_vectors(x, y, z, shp):
+    """The 1-D coordinate vectors if x, y, z are per-axis arrays of shapes
+    (n,1,1), (1,n,1), (1,1,n) (how material_and_flags calls the labels)."""
+    try:
+        if (len(shp) == 3 and np.shape(x) == (shp[0], 1, 1) and np.shape(y) == (1, shp[1], 1)
+                and np.shape(z) == (1, 1, shp[2])):
+            return np.ravel(x), np.ravel(y), np.ravel(z)
+    except Exception:
+        pass
+    return None
 
 
 def single_sphere(n=32, voxel_nm=1.25, diameter_nm=36.0, box_nm=None, eps_physics=-4.42 + 0.21j,
