@@ -227,6 +227,31 @@ def run_gpu(args, rank, world, local_rank):
                     true_residual=true_residual)
         return r
 
+    if args.only_matvec:
+        # operator applications only (profiling entry): FP32 then FP64, W warm-up + K timed each
+        res = {}
+        for name, dt, prec in (("fp32", torch.complex64, V.PREC_MIXED), ("fp64", torch.complex128, V.PREC_FP64)):
+            x = torch.randn((3,) + w.shape, dtype=dt, device="cuda")
+            y = torch.zeros_like(x)
+            torch.cuda.synchronize()
+            for _ in range(args.warmup):
+                c.matvec_dev(x.data_ptr(), y.data_ptr(), precision=prec)
+            c.sync()
+            a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a0.record(stream)
+            for _ in range(args.steps):
+                c.matvec_dev(x.data_ptr(), y.data_ptr(), precision=prec)
+            a1.record(stream)
+            a1.synchronize()
+            ms = a0.elapsed_time(a1) / args.steps
+            B = bytes_per_matvec(w.shape, 8 if name == "fp32" else 16)
+            res[name] = {"ms": ms, "GBps": B / ms / 1e6, "hbm_frac": B / ms / 1e6 / measured_peaks()[0]}
+            del x, y
+        if rank == 0:
+            print(json.dumps({"mode": "matvec", "workload": args.workload, "grid": list(w.shape), **res}), flush=True)
+        c.close()
+        return
+
     # ---- warm-up
     for _ in range(args.warmup):
         last = solve(V.PREC_MIXED)
@@ -383,6 +408,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--fp64-iters", type=int, default=0)
+    ap.add_argument("--only-matvec", action="store_true",
+                    help="time operator applications only (FP32 and FP64), no solve")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
