@@ -100,6 +100,18 @@ VIE_API int vie_set_rhs(vie_ctx* ctx, const double* e);
    X_FFT/Y_FFT/Z_FFT (CG_Iteration.h:131-173) or the _Conjugate twins
    (:86-128), then Current_Reset (fft.h:13-35). */
 VIE_API int vie_matvec(vie_ctx* ctx, const double* x, double* y, int conj);
+/* Same as vie_matvec (FP64, host buffers), but it allocates no device memory.
+   No counterpart in the reference.  For callers that must not allocate while
+   they apply the operator: code that calls it inside a long loop, where the
+   cudaMalloc/cudaFree pair of vie_matvec would synchronise the whole device
+   each time, or a process whose free device memory is held by another
+   allocator, where a new cudaMalloc can fail.  The device copies of x and y
+   and the pass scratch live in one static 64 MiB device array per GPU, so the
+   grid may have at most 174762 voxels (VIE_ERR_ARG beyond that).  All calls on
+   a GPU share that array: calls that overlap on one GPU race and must be
+   serialised by the caller.  The first call on a device looks up the array's
+   device address; make it before any stream capture. */
+VIE_API int vie_matvec_static(vie_ctx* ctx, const double* x, double* y, int conj);
 /* Same on device buffers of the context's GPU.  precision VIE_PREC_FP64:
    x, y are 3a double2; VIE_PREC_MIXED: 3a float2 (the FP32 operator).
    Runs on the context stream; returns after the launch (no sync). */
