@@ -1,0 +1,425 @@
+// vie_fast.cuh -- register-resident four-step pencil FFT passes for the common
+// axis lengths (compile-time N = R1 * R2).
+//
+// Each length-N transform is done as
+//     X[k1 + R1 k2] = sum_n2 W_R2^{n2 k2} W_N^{n2 k1} sum_n1 x[n2 + R2 n1] W_R1^{n1 k1}
+// step A: thread "n2" loads its R1 inputs (stride R2), DFT_R1 in registers,
+//         twiddles W_N^{n2 k1}, one shared-memory transpose;
+// step B: thread "k1" reads its R2 values, DFT_R2 in registers and holds
+//         X[k1 + R1 k2], k2 < R2: a natural-order spectrum, strided over threads.
+// The inverse runs the same two steps backwards with conjugate twiddles.
+// Padding split as in vie_operator.cuh: the even half transforms x, the odd
+// half x . W_2N^n; the inverse crop combines y = y_even + W_2N^{-n} y_odd.
+//
+// Spectral slot orders these kernels use: z natural (slot = k); x and y
+// "half-natural" (slot = h N + m for spectral index k = 2m + h).
+//
+// All index arithmetic is compile-time except the tile origins; thread roles:
+//   column passes (pencils contiguous in memory): tid = lane * TP + tx,
+//   row passes (pencils are contiguous rows):     tid = row * L + lane.
+#pragma once
+#include "vie_operator.cuh"
+
+namespace vie {
+
+template <int N> struct FastPlan { static constexpr bool ok = false; static constexpr int R1 = 1, R2 = 1; };
+template <> struct FastPlan<256> { static constexpr bool ok = true; static constexpr int R1 = 16, R2 = 16; };
+template <> struct FastPlan<128> { static constexpr bool ok = true; static constexpr int R1 = 16, R2 = 8; };
+template <> struct FastPlan<64> { static constexpr bool ok = true; static constexpr int R1 = 8, R2 = 8; };
+template <> struct FastPlan<32> { static constexpr bool ok = true; static constexpr int R1 = 8, R2 = 4; };
+template <> struct FastPlan<16> { static constexpr bool ok = true; static constexpr int R1 = 4, R2 = 4; };
+
+inline bool fast_length(int n) { return n == 256 || n == 128 || n == 64 || n == 32 || n == 16; }
+
+template <int R, bool INV, typename C> __device__ __forceinline__ void dft_reg(C* v) {
+    if constexpr (R == 2) dft2<INV>(v[0], v[1]);
+    else if constexpr (R == 4) dft4<INV>(v[0], v[1], v[2], v[3]);
+    else if constexpr (R == 8) dft8<INV>(v);
+    else if constexpr (R == 16) dft16<INV>(v);
+    else static_assert(R == 2, "unsupported register radix");
+}
+
+// pencils per CTA of the column passes (one row segment of TP * sizeof(C) bytes)
+template <typename C> struct FastTiles;
+template <> struct FastTiles<float2> { static constexpr int TP_Y = 16, TP_X = 8, ROWS_DIV = 1; };
+template <> struct FastTiles<double2> { static constexpr int TP_Y = 8, TP_X = 4, ROWS_DIV = 2; };
+
+// shared memory layout: [tw 2N][buffer]
+template <typename C, int N> __device__ __forceinline__ C* fast_smem(const C* gtw, C*& tw) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    tw = reinterpret_cast<C*>(smem_raw);
+    for (int u = threadIdx.x; u < 2 * N; u += blockDim.x) tw[u] = gtw[u];
+    return tw + 2 * N;
+}
+
+template <typename C, int N> __host__ __device__ constexpr int fast_lanes() {
+    return FastPlan<N>::R1 > FastPlan<N>::R2 ? FastPlan<N>::R1 : FastPlan<N>::R2;
+}
+template <typename C, int N> __host__ __device__ constexpr int fast_rows() {
+    return (256 / fast_lanes<C, N>()) / FastTiles<C>::ROWS_DIV;
+}
+
+template <typename C, int N> __host__ __device__ constexpr size_t fast_smem_row() {
+    // E[2][R1 or R2][ROWS][R+1]
+    constexpr int R1 = FastPlan<N>::R1, R2 = FastPlan<N>::R2;
+    constexpr int A = R1 * (R2 + 1) > R2 * (R1 + 1) ? R1 * (R2 + 1) : R2 * (R1 + 1);
+    return sizeof(C) * (2 * (size_t)N + 2 * (size_t)A * fast_rows<C, N>());
+}
+template <typename C, int N> __host__ __device__ constexpr size_t fast_smem_col() {
+    return sizeof(C) * (2 * (size_t)N + 2 * (size_t)N * FastTiles<C>::TP_Y);
+}
+template <typename C, int N> __host__ __device__ constexpr size_t fast_smem_x() {
+    return sizeof(C) * (2 * (size_t)N + 6 * (size_t)N * FastTiles<C>::TP_X);
+}
+
+// ---------------------------------------------------------------------------
+// F1 (row pass): forward z with padding fused into the load.
+// E layout: E[h][k1][row][n2] with row stride (R2 + 1).
+// ---------------------------------------------------------------------------
+template <typename C, int N, class Pro>
+__global__ void __launch_bounds__(256) kf_fwd_z(OpDev<C> op, Pro pro) {
+    constexpr int R1 = FastPlan<N>::R1, R2 = FastPlan<N>::R2, L = fast_lanes<C, N>(), ROWS = fast_rows<C, N>();
+    constexpr int SR = R2 + 1;                 // padded row of E
+    constexpr int HS = R1 * ROWS * SR;         // one half
+    C* tw;
+    C* E = fast_smem<C, N>(op.ax[2].tw, tw);
+    const int lane = threadIdx.x % L, r = threadIdx.x / L;
+    const int s = blockIdx.y;
+    const long long nrows = (long long)op.nx * op.ny;
+    const long long row = (long long)blockIdx.x * ROWS + r;
+    const bool live = row < nrows;
+    __syncthreads();
+    if (lane < R2 && live) {
+        const int n2 = lane;
+        const int i = (int)(row / op.ny), j = (int)(row - (long long)i * op.ny);
+        const bool vrow = (s != 0 || i < op.nx - 1) && (s != 1 || j < op.ny - 1);
+        C v[R1];
+#pragma unroll
+        for (int n1 = 0; n1 < R1; n1++) {
+            const int n = n2 + R2 * n1;
+            const bool valid = vrow && (s != 2 || n < N - 1);
+            C x = pro(s, row * N + n, valid);
+            v[n1] = valid ? x : czero<C>();
+        }
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            C a[R1];
+#pragma unroll
+            for (int n1 = 0; n1 < R1; n1++) a[n1] = h ? cmul(v[n1], tw[n2 + R2 * n1]) : v[n1];
+            dft_reg<R1, false>(a);
+#pragma unroll
+            for (int k1 = 0; k1 < R1; k1++) {
+                const C t = k1 ? cmul(a[k1], tw[2 * n2 * k1]) : a[k1];
+                E[h * HS + (k1 * ROWS + r) * SR + n2] = t;
+            }
+        }
+    }
+    __syncthreads();
+    if (lane < R1 && live) {
+        const int k1 = lane;
+        C X[2][R2];
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+#pragma unroll
+            for (int n2 = 0; n2 < R2; n2++) X[h][n2] = E[h * HS + (k1 * ROWS + r) * SR + n2];
+            dft_reg<R2, false>(X[h]);
+        }
+        C* dst = op.b + ((long long)s * nrows + row) * (2 * N);
+#pragma unroll
+        for (int k2 = 0; k2 < R2; k2++) {
+            const int m = k1 + R1 * k2;
+            dst[2 * m] = X[0][k2];
+            dst[2 * m + 1] = X[1][k2];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// I1 (row pass): inverse z, crop, diagonal term, mask, epilogue.
+// E layout: E[h][n2][row][k1] with row stride (R1 + 1).
+// ---------------------------------------------------------------------------
+template <typename C, int N, bool CONJ, class Epi>
+__global__ void __launch_bounds__(256) kf_inv_z(OpDev<C> op, const C* __restrict__ xin, Epi epi,
+                                                double2* __restrict__ partial) {
+    using R = typename real_of<C>::type;
+    constexpr int R1 = FastPlan<N>::R1, R2 = FastPlan<N>::R2, L = fast_lanes<C, N>(), ROWS = fast_rows<C, N>();
+    constexpr int SR = R1 + 1;
+    constexpr int HS = R2 * ROWS * SR;
+    C* tw;
+    C* E = fast_smem<C, N>(op.ax[2].tw, tw);
+    const int lane = threadIdx.x % L, r = threadIdx.x / L;
+    const int s = blockIdx.y;
+    const long long nrows = (long long)op.nx * op.ny;
+    const long long row = (long long)blockIdx.x * ROWS + r;
+    const bool live = row < nrows;
+    __syncthreads();
+    if (lane < R1 && live) {
+        const int k1 = lane;
+        const C* src = op.b + ((long long)s * nrows + row) * (2 * N);
+        C X[2][R2];
+#pragma unroll
+        for (int k2 = 0; k2 < R2; k2++) {
+            const int m = k1 + R1 * k2;
+            X[0][k2] = src[2 * m];
+            X[1][k2] = src[2 * m + 1];
+        }
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            dft_reg<R2, true>(X[h]);
+#pragma unroll
+            for (int n2 = 0; n2 < R2; n2++) {
+                const C t = n2 ? cmulc(X[h][n2], tw[2 * n2 * k1]) : X[h][n2];
+                E[h * HS + (n2 * ROWS + r) * SR + k1] = t;
+            }
+        }
+    }
+    __syncthreads();
+    constexpr int KA = Epi::K > 0 ? Epi::K : 1;
+    double2 acc[KA];
+#pragma unroll
+    for (int k = 0; k < KA; k++) acc[k] = make_double2(0.0, 0.0);
+    if (lane < R2 && live) {
+        const int n2 = lane;
+        C y0[R1], y1[R1];
+#pragma unroll
+        for (int k1 = 0; k1 < R1; k1++) {
+            y0[k1] = E[(n2 * ROWS + r) * SR + k1];
+            y1[k1] = E[HS + (n2 * ROWS + r) * SR + k1];
+        }
+        dft_reg<R1, true>(y0);
+        dft_reg<R1, true>(y1);
+        const int i = (int)(row / op.ny), j = (int)(row - (long long)i * op.ny);
+        const bool vrow = (s != 0 || i < op.nx - 1) && (s != 1 || j < op.ny - 1);
+        const long long sstep = s == 0 ? (long long)op.ny * N : (s == 1 ? (long long)N : 1LL);
+        const R dc = op.dcoef[s];
+#pragma unroll
+        for (int n1 = 0; n1 < R1; n1++) {
+            const int n = n2 + R2 * n1;
+            const long long idx = row * N + n;
+            C y = czero<C>();
+            if ((op.flags[idx] >> s) & 1) {
+                y = cadd(y0[n1], cmulc(y1[n1], tw[n]));
+                if (vrow && (s != 2 || n < N - 1)) {
+                    const C ws = cadd(op.w[idx + sstep], op.w[idx]);
+                    C coef = mkc(-dc * ws.y, dc * ws.x);
+                    if (CONJ) coef = cconj(coef);
+                    y = cadd(y, cmul(coef, xin[(long long)s * op.a + idx]));
+                }
+            }
+            epi(s, idx, y, acc);
+        }
+    }
+    if constexpr (Epi::K > 0) block_reduce_store<KA>(acc, partial, (long long)blockIdx.y * gridDim.x + blockIdx.x);
+}
+
+// ---------------------------------------------------------------------------
+// F2 (column pass): forward y.  grid (kz tiles of TP, nx, 3).
+// E layout: E[h][k1][n2][tx].
+// ---------------------------------------------------------------------------
+template <typename C, int N>
+__global__ void __launch_bounds__(256) kf_fwd_y(OpDev<C> op) {
+    constexpr int R1 = FastPlan<N>::R1, R2 = FastPlan<N>::R2, TP = FastTiles<C>::TP_Y;
+    constexpr int HS = N * TP;
+    C* tw;
+    C* E = fast_smem<C, N>(op.ax[1].tw, tw);
+    const int tx = threadIdx.x % TP, lane = threadIdx.x / TP;
+    const int Lz = 2 * op.nz;
+    const int kz = blockIdx.x * TP + tx, i = blockIdx.y, s = blockIdx.z;
+    const bool live = kz < Lz;
+    const C* src = op.b + ((long long)s * op.nx + i) * (long long)N * Lz;
+    __syncthreads();
+    if (lane < R2 && live) {
+        const int n2 = lane;
+        C v[R1];
+#pragma unroll
+        for (int n1 = 0; n1 < R1; n1++) v[n1] = src[(long long)(n2 + R2 * n1) * Lz + kz];
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            C a[R1];
+#pragma unroll
+            for (int n1 = 0; n1 < R1; n1++) a[n1] = h ? cmul(v[n1], tw[n2 + R2 * n1]) : v[n1];
+            dft_reg<R1, false>(a);
+#pragma unroll
+            for (int k1 = 0; k1 < R1; k1++)
+                E[h * HS + (k1 * R2 + n2) * TP + tx] = k1 ? cmul(a[k1], tw[2 * n2 * k1]) : a[k1];
+        }
+    }
+    __syncthreads();
+    if (lane < R1 && live) {
+        const int k1 = lane;
+        C* dst = op.c + ((long long)s * op.nx + i) * (long long)(2 * N) * Lz;
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            C X[R2];
+#pragma unroll
+            for (int n2 = 0; n2 < R2; n2++) X[n2] = E[h * HS + (k1 * R2 + n2) * TP + tx];
+            dft_reg<R2, false>(X);
+#pragma unroll
+            for (int k2 = 0; k2 < R2; k2++) dst[(long long)(h * N + k1 + R1 * k2) * Lz + kz] = X[k2];
+        }
+    }
+}
+
+// I2 (column pass): inverse y, crop.  E layout: E[h][n2][k1][tx].
+template <typename C, int N>
+__global__ void __launch_bounds__(256) kf_inv_y(OpDev<C> op) {
+    constexpr int R1 = FastPlan<N>::R1, R2 = FastPlan<N>::R2, TP = FastTiles<C>::TP_Y;
+    constexpr int HS = N * TP;
+    C* tw;
+    C* E = fast_smem<C, N>(op.ax[1].tw, tw);
+    const int tx = threadIdx.x % TP, lane = threadIdx.x / TP;
+    const int Lz = 2 * op.nz;
+    const int kz = blockIdx.x * TP + tx, i = blockIdx.y, s = blockIdx.z;
+    const bool live = kz < Lz;
+    const C* src = op.c + ((long long)s * op.nx + i) * (long long)(2 * N) * Lz;
+    __syncthreads();
+    if (lane < R1 && live) {
+        const int k1 = lane;
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            C X[R2];
+#pragma unroll
+            for (int k2 = 0; k2 < R2; k2++) X[k2] = src[(long long)(h * N + k1 + R1 * k2) * Lz + kz];
+            dft_reg<R2, true>(X);
+#pragma unroll
+            for (int n2 = 0; n2 < R2; n2++)
+                E[h * HS + (n2 * R1 + k1) * TP + tx] = n2 ? cmulc(X[n2], tw[2 * n2 * k1]) : X[n2];
+        }
+    }
+    __syncthreads();
+    if (lane < R2 && live) {
+        const int n2 = lane;
+        C y0[R1], y1[R1];
+#pragma unroll
+        for (int k1 = 0; k1 < R1; k1++) {
+            y0[k1] = E[(n2 * R1 + k1) * TP + tx];
+            y1[k1] = E[HS + (n2 * R1 + k1) * TP + tx];
+        }
+        dft_reg<R1, true>(y0);
+        dft_reg<R1, true>(y1);
+        C* dst = op.b + ((long long)s * op.nx + i) * (long long)N * Lz;
+#pragma unroll
+        for (int n1 = 0; n1 < R1; n1++) {
+            const int n = n2 + R2 * n1;
+            dst[(long long)n * Lz + kz] = cadd(y0[n1], cmulc(y1[n1], tw[n]));
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// F3 (column pass, three components): forward x, spectral multiply, inverse x,
+// crop.  grid (kz tiles of TP, 2ny).  E layout: E[s][h][k1][n2][tx] (forward)
+// then E[s][h][k1][k2][tx] (spectra) then E[s][h][k1][n2][tx] (inverse).
+// Thread roles: steps A/A' (tx, s, n2); step B / multiply / B' (tx, h, k1).
+// ---------------------------------------------------------------------------
+template <typename C, int N, bool CONJ>
+__global__ void __launch_bounds__(384) kf_x_spectral(OpDev<C> op) {
+    using R = typename real_of<C>::type;
+    constexpr int R1 = FastPlan<N>::R1, R2 = FastPlan<N>::R2, TP = FastTiles<C>::TP_X;
+    constexpr int L = R1 > R2 ? R1 : R2;
+    constexpr int HS = N * TP, SS = 2 * HS;
+    C* tw;
+    C* E = fast_smem<C, N>(op.ax[0].tw, tw);
+    const int Lz = 2 * op.nz, Ly = 2 * op.ny;
+    const int ky = blockIdx.y;
+    const long long cs = (long long)Ly * Lz;
+    const int tx = threadIdx.x % TP;
+    const int kz = blockIdx.x * TP + tx;
+    const bool live = kz < Lz;
+    __syncthreads();
+    // step A: thread (tx, s, n2)
+    {
+        const int q = threadIdx.x / TP;  // 0 .. 3L-1
+        const int s = q / L, n2 = q % L;
+        if (s < 3 && n2 < R2 && live) {
+            C v[R1];
+#pragma unroll
+            for (int n1 = 0; n1 < R1; n1++)
+                v[n1] = op.c[((long long)s * N + n2 + R2 * n1) * cs + (long long)ky * Lz + kz];
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                C a[R1];
+#pragma unroll
+                for (int n1 = 0; n1 < R1; n1++) a[n1] = h ? cmul(v[n1], tw[n2 + R2 * n1]) : v[n1];
+                dft_reg<R1, false>(a);
+#pragma unroll
+                for (int k1 = 0; k1 < R1; k1++)
+                    E[s * SS + h * HS + (k1 * R2 + n2) * TP + tx] = k1 ? cmul(a[k1], tw[2 * n2 * k1]) : a[k1];
+            }
+        }
+    }
+    __syncthreads();
+    // step B, multiply, step B': thread (tx, h, k1); every element it touches is its own
+    {
+        const int q = threadIdx.x / TP;
+        const int h = q / R1, k1 = q % R1;
+        if (h < 2 && live) {
+            const int md = CONJ ? 1 : 0;
+            C* base = E + h * HS + (k1 * R2) * TP + tx;  // + s*SS + k2*TP
+#pragma unroll
+            for (int s = 0; s < 3; s++) {
+                C X[R2];
+#pragma unroll
+                for (int n2 = 0; n2 < R2; n2++) X[n2] = base[s * SS + n2 * TP];
+                dft_reg<R2, false>(X);
+#pragma unroll
+                for (int k2 = 0; k2 < R2; k2++) base[s * SS + k2 * TP] = X[k2];
+            }
+            const C Py = op.ax[1].P[md][ky], Qy = op.ax[1].Q[md][ky];
+            const int gy = op.ax[1].gfold[ky];
+            const C Pz = op.ax[2].P[md][kz], Qz = op.ax[2].Q[md][kz];
+            const int gz = op.ax[2].gfold[kz];
+            const R kx_ = op.kappa[0], ky_ = op.kappa[1], kz_ = op.kappa[2];
+#pragma unroll 4
+            for (int k2 = 0; k2 < R2; k2++) {
+                const int sx = h * N + k1 + R1 * k2;
+                const C Px = op.ax[0].P[md][sx], Qx = op.ax[0].Q[md][sx];
+                const int gx = op.ax[0].gfold[sx];
+                C G = op.Gs[((long long)gx * (op.ny + 1) + gy) * (op.nz + 1) + gz];
+                if (CONJ) G = cconj(G);
+                C* e = base + k2 * TP;
+                const C Jx = e[0], Jy = e[SS], Jz = e[2 * SS];
+                const C rho = cadd(cadd(cmul(Px, Jx), cmul(Py, Jy)), cmul(Pz, Jz));
+                e[0] = cmul(G, cadd(cscale(Jx, kx_), cmul(Qx, rho)));
+                e[SS] = cmul(G, cadd(cscale(Jy, ky_), cmul(Qy, rho)));
+                e[2 * SS] = cmul(G, cadd(cscale(Jz, kz_), cmul(Qz, rho)));
+            }
+#pragma unroll
+            for (int s = 0; s < 3; s++) {
+                C X[R2];
+#pragma unroll
+                for (int k2 = 0; k2 < R2; k2++) X[k2] = base[s * SS + k2 * TP];
+                dft_reg<R2, true>(X);
+#pragma unroll
+                for (int n2 = 0; n2 < R2; n2++) base[s * SS + n2 * TP] = n2 ? cmulc(X[n2], tw[2 * n2 * k1]) : X[n2];
+            }
+        }
+    }
+    __syncthreads();
+    // step A': thread (tx, s, n2)
+    {
+        const int q = threadIdx.x / TP;
+        const int s = q / L, n2 = q % L;
+        if (s < 3 && n2 < R2 && live) {
+            C y0[R1], y1[R1];
+#pragma unroll
+            for (int k1 = 0; k1 < R1; k1++) {
+                y0[k1] = E[s * SS + (k1 * R2 + n2) * TP + tx];
+                y1[k1] = E[s * SS + HS + (k1 * R2 + n2) * TP + tx];
+            }
+            dft_reg<R1, true>(y0);
+            dft_reg<R1, true>(y1);
+#pragma unroll
+            for (int n1 = 0; n1 < R1; n1++) {
+                const int n = n2 + R2 * n1;
+                op.c[((long long)s * N + n) * cs + (long long)ky * Lz + kz] = cadd(y0[n1], cmulc(y1[n1], tw[n]));
+            }
+        }
+    }
+}
+
+template <typename C, int N> constexpr int fast_x_threads() {
+    return 3 * (FastPlan<N>::R1 > FastPlan<N>::R2 ? FastPlan<N>::R1 : FastPlan<N>::R2) * FastTiles<C>::TP_X;
+}
+
+}  // namespace vie

@@ -3,6 +3,7 @@
 #include <mutex>
 #include <unordered_map>
 
+#include "vie_fast.cuh"
 #include "vie_internal.h"
 
 namespace vie {
@@ -30,12 +31,90 @@ inline unsigned ceil_div(long long a, long long b) { return (unsigned)((a + b - 
 
 // Number of blocks of the last pass (rows of the reduction partials).
 template <typename T> inline long long epilogue_blocks(const Operator<T>& op) {
-    return (long long)ceil_div((long long)op.dev.nx * op.dev.ny, op.dev.tz) * 3;
+    using C = cplx_t<T>;
+    const long long nrows = (long long)op.dev.nx * op.dev.ny;
+    int rows = op.dev.tz;
+    if (op.dev.fast[2]) {
+        switch (op.dev.nz) {
+            case 256: rows = fast_rows<C, 256>(); break;
+            case 128: rows = fast_rows<C, 128>(); break;
+            case 64: rows = fast_rows<C, 64>(); break;
+            case 32: rows = fast_rows<C, 32>(); break;
+            case 16: rows = fast_rows<C, 16>(); break;
+        }
+    }
+    return (long long)ceil_div(nrows, rows) * 3;
 }
+
+// fast z passes for a compile-time N
+template <typename T, int N, class Pro, class Epi>
+int launch_fast_z(Operator<T>& op, bool forward, Pro pro, Epi epi, const cplx_t<T>* xdiag, bool conj,
+                  double2* partial, cudaStream_t st, Error& err) {
+    using C = cplx_t<T>;
+    constexpr int ROWS = fast_rows<C, N>(), L = fast_lanes<C, N>();
+    constexpr size_t smem = fast_smem_row<C, N>();
+    const long long nrows = (long long)op.dev.nx * op.dev.ny;
+    dim3 grid(ceil_div(nrows, ROWS), 3);
+    if (forward) {
+        auto kf = kf_fwd_z<C, N, Pro>;
+        VIE_CUDA_TRY(ensure_smem(kf, smem), err);
+        kf<<<grid, L * ROWS, smem, st>>>(op.dev, pro);
+        count_launch();
+    } else if (conj) {
+        auto kf = kf_inv_z<C, N, true, Epi>;
+        VIE_CUDA_TRY(ensure_smem(kf, smem), err);
+        kf<<<grid, L * ROWS, smem, st>>>(op.dev, xdiag, epi, partial);
+        count_launch();
+    } else {
+        auto kf = kf_inv_z<C, N, false, Epi>;
+        VIE_CUDA_TRY(ensure_smem(kf, smem), err);
+        kf<<<grid, L * ROWS, smem, st>>>(op.dev, xdiag, epi, partial);
+        count_launch();
+    }
+    return VIE_OK;
+}
+
+template <typename T, int N>
+int launch_fast_y(Operator<T>& op, bool forward, cudaStream_t st, Error& err) {
+    using C = cplx_t<T>;
+    constexpr int TP = FastTiles<C>::TP_Y, L = fast_lanes<C, N>();
+    constexpr size_t smem = fast_smem_col<C, N>();
+    dim3 grid(ceil_div(2 * op.dev.nz, TP), op.dev.nx, 3);
+    auto kf = forward ? kf_fwd_y<C, N> : kf_inv_y<C, N>;
+    VIE_CUDA_TRY(ensure_smem(kf, smem), err);
+    kf<<<grid, TP * L, smem, st>>>(op.dev);
+    count_launch();
+    return VIE_OK;
+}
+
+template <typename T, int N>
+int launch_fast_x(Operator<T>& op, bool conj, cudaStream_t st, Error& err) {
+    using C = cplx_t<T>;
+    constexpr int TP = FastTiles<C>::TP_X;
+    constexpr size_t smem = fast_smem_x<C, N>();
+    dim3 grid(ceil_div(2 * op.dev.nz, TP), 2 * op.dev.ny);
+    auto kf = conj ? kf_x_spectral<C, N, true> : kf_x_spectral<C, N, false>;
+    VIE_CUDA_TRY(ensure_smem(kf, smem), err);
+    kf<<<grid, fast_x_threads<C, N>(), smem, st>>>(op.dev);
+    count_launch();
+    return VIE_OK;
+}
+
+#define VIE_FAST_SWITCH(n, CALL)                             \
+    switch (n) {                                              \
+        case 256: { constexpr int NN = 256; CALL; } break;    \
+        case 128: { constexpr int NN = 128; CALL; } break;    \
+        case 64: { constexpr int NN = 64; CALL; } break;      \
+        case 32: { constexpr int NN = 32; CALL; } break;      \
+        case 16: { constexpr int NN = 16; CALL; } break;      \
+        default: break;                                       \
+    }
 
 // y = A x (or A^H x) with a prologue producing the source values and an
 // epilogue consuming the outputs.  xdiag is the source vector the diagonal
-// term reads (the same values the prologue returns where valid).
+// term reads (the same values the prologue returns where valid).  Each axis
+// runs the register four-step kernels when its length is one of the
+// compile-time lengths, the generic shared-memory kernels otherwise.
 template <typename T, class Pro, class Epi>
 int launch_operator(Operator<T>& op, Pro pro, Epi epi, const cplx_t<T>* xdiag, bool conj, double2* partial,
                     cudaStream_t st, Error& err) {
@@ -43,19 +122,31 @@ int launch_operator(Operator<T>& op, Pro pro, Epi epi, const cplx_t<T>* xdiag, b
     const OpDev<C>& d = op.dev;
     const long long nrows = (long long)d.nx * d.ny;
     const int Lz = 2 * d.nz, Ly = 2 * d.ny;
-    {
+    int rc = VIE_OK;
+    // F1
+    if (d.fast[2]) {
+        VIE_FAST_SWITCH(d.nz, rc = (launch_fast_z<T, NN, Pro, Epi>(op, true, pro, epi, xdiag, conj, partial, st, err)));
+    } else {
         auto kf = k_fwd_z<C, Pro>;
         VIE_CUDA_TRY(ensure_smem(kf, op.smem_z), err);
         kf<<<dim3(ceil_div(nrows, d.tz), 3), kThreads, op.smem_z, st>>>(d, pro);
         count_launch();
     }
-    {
+    if (rc) return rc;
+    // F2
+    if (d.fast[1]) {
+        VIE_FAST_SWITCH(d.ny, rc = (launch_fast_y<T, NN>(op, true, st, err)));
+    } else {
         auto kf = k_fwd_y<C>;
         VIE_CUDA_TRY(ensure_smem(kf, op.smem_y), err);
         kf<<<dim3(ceil_div(Lz, d.tc), d.nx, 3), kThreads, op.smem_y, st>>>(d);
         count_launch();
     }
-    if (conj) {
+    if (rc) return rc;
+    // F3
+    if (d.fast[0]) {
+        VIE_FAST_SWITCH(d.nx, rc = (launch_fast_x<T, NN>(op, conj, st, err)));
+    } else if (conj) {
         auto kf = k_x_spectral<C, true>;
         VIE_CUDA_TRY(ensure_smem(kf, op.smem_x), err);
         kf<<<dim3(ceil_div(Lz, d.tx), Ly), kThreads, op.smem_x, st>>>(d);
@@ -66,13 +157,21 @@ int launch_operator(Operator<T>& op, Pro pro, Epi epi, const cplx_t<T>* xdiag, b
         kf<<<dim3(ceil_div(Lz, d.tx), Ly), kThreads, op.smem_x, st>>>(d);
         count_launch();
     }
-    {
+    if (rc) return rc;
+    // I2
+    if (d.fast[1]) {
+        VIE_FAST_SWITCH(d.ny, rc = (launch_fast_y<T, NN>(op, false, st, err)));
+    } else {
         auto kf = k_inv_y<C>;
         VIE_CUDA_TRY(ensure_smem(kf, op.smem_y), err);
         kf<<<dim3(ceil_div(Lz, d.tc), d.nx, 3), kThreads, op.smem_y, st>>>(d);
         count_launch();
     }
-    if (conj) {
+    if (rc) return rc;
+    // I1
+    if (d.fast[2]) {
+        VIE_FAST_SWITCH(d.nz, rc = (launch_fast_z<T, NN, Pro, Epi>(op, false, pro, epi, xdiag, conj, partial, st, err)));
+    } else if (conj) {
         auto kf = k_inv_z<C, true, Epi>;
         VIE_CUDA_TRY(ensure_smem(kf, op.smem_z), err);
         kf<<<dim3(ceil_div(nrows, d.tz), 3), kThreads, op.smem_z, st>>>(d, xdiag, epi, partial);
@@ -83,6 +182,7 @@ int launch_operator(Operator<T>& op, Pro pro, Epi epi, const cplx_t<T>* xdiag, b
         kf<<<dim3(ceil_div(nrows, d.tz), 3), kThreads, op.smem_z, st>>>(d, xdiag, epi, partial);
         count_launch();
     }
+    if (rc) return rc;
     VIE_CUDA_TRY(cudaGetLastError(), err);
     return VIE_OK;
 }

@@ -1,6 +1,7 @@
 // vie_operator.cu -- host setup of the operator: radix plans, per-axis tables,
 // Green octant scaling, contrast upload, scratch, and the plain matvec.
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 #include "vie_launch.cuh"
@@ -94,6 +95,10 @@ int Operator<T>::init(int nx, int ny, int nz, const double d[3], double k0, cons
     }
     const int n[3] = {nx, ny, nz};
     for (int ax = 0; ax < 3; ax++) o.plan[ax] = plans[ax];
+    // register four-step kernels for the compile-time lengths (VIE_FAST=0 forces the generic ones)
+    const char* fe = std::getenv("VIE_FAST");
+    const bool allow_fast = !(fe && fe[0] == '0');
+    for (int ax = 0; ax < 3; ax++) o.fast[ax] = (allow_fast && fast_length(n[ax])) ? 1 : 0;
 
     // ---- tables: per axis tw[2N], perm[N] (u16), P[2][2N], Q[2][2N], gfold[2N]
     size_t bytes = 0;
@@ -132,6 +137,9 @@ int Operator<T>::init(int nx, int ny, int nz, const double d[3], double k0, cons
             int k;
             if (ax == 2) {
                 k = slot;  // z spectra are stored in natural order
+            } else if (o.fast[ax]) {
+                const int hh = slot >= N ? 1 : 0;
+                k = 2 * (slot - hh * N) + hh;  // half-natural: slot = h N + m, k = 2m + h
             } else {
                 const int hh = slot >= N ? 1 : 0;
                 k = 2 * dr[slot - hh * N] + hh;

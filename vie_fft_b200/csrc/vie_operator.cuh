@@ -50,6 +50,7 @@ template <typename C> struct OpDev {
     const C* Gs;               // (nx+1)(ny+1)(nz+1) octant, scaled
     const C* w;                // per voxel 1/(eps-1)
     const unsigned char* flags;  // bit0 Flag_X, bit1 Flag_Y, bit2 Flag_Z
+    int fast[3];               // axis uses the register four-step kernels (half-natural slots)
     typename real_of<C>::type kappa[3];   // k0^2 delta_f
     typename real_of<C>::type dcoef[3];   // -delta_f Z0 / (2 k0)
     C* b;                      // 3 * nx*ny*2nz scratch
