@@ -54,7 +54,9 @@ extern "C" {
 
 /* arithmetic of a solve */
 #define VIE_PREC_FP64 0   /* every operation in FP64 complex */
-#define VIE_PREC_MIXED 1  /* FP32-complex inner Krylov inside FP64 defect correction */
+#define VIE_PREC_MIXED 1  /* FP32-complex Krylov with FP64 defect correction: BiCGSTAB
+                             folds in FP64 true residuals (reliable updates), the other
+                             drivers restart an FP32 inner solve per FP64 refinement */
 
 typedef struct vie_ctx vie_ctx;
 
@@ -122,7 +124,9 @@ typedef struct {
     int precision;      /* VIE_PREC_FP64 or VIE_PREC_MIXED */
     double tol;         /* relative-residual threshold (CG_THR, CG_Iteration.h:46) */
     int max_iter;       /* iteration cap; <= 0 means nx*ny*nz like the reference */
-    double inner_tol;   /* mixed: inner reduction per refinement step (<= 0: 1e-4) */
+    double inner_tol;   /* mixed: residual reduction per FP64 refinement step
+                           (<= 0: 0.1 for BiCGSTAB's reliable updates, 1e-4 for the
+                           restarted inner solves of the other drivers) */
     int max_outer;      /* mixed: refinement cap (<= 0: 30) */
     int verbose;        /* print "CG Error" per iteration like the reference */
     int true_residual;  /* FP64 solves: evaluate ||b - A x|| / ||b|| at exit (one more

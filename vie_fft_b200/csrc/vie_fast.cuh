@@ -60,27 +60,40 @@ template <typename C, int N> __host__ __device__ constexpr int fast_rows() {
 }
 
 template <typename C, int N> __host__ __device__ constexpr size_t fast_smem_row() {
-    // E[2][R1 or R2][ROWS][R+1]
+    // E[2][ROWS][R][R'+1]: rows outermost, padded inner rows (bank-conflict free)
     constexpr int R1 = FastPlan<N>::R1, R2 = FastPlan<N>::R2;
     constexpr int A = R1 * (R2 + 1) > R2 * (R1 + 1) ? R1 * (R2 + 1) : R2 * (R1 + 1);
     return sizeof(C) * (2 * (size_t)N + 2 * (size_t)A * fast_rows<C, N>());
+}
+// x pass: E[3][2][R1][R2*TP + TP] (each k1 block padded by TP entries)
+template <typename C, int N> __host__ __device__ constexpr int fast_x_kstride() {
+    return FastPlan<N>::R2 * FastTiles<C>::TP_X + FastTiles<C>::TP_X;
 }
 template <typename C, int N> __host__ __device__ constexpr size_t fast_smem_col() {
     return sizeof(C) * (2 * (size_t)N + 2 * (size_t)N * FastTiles<C>::TP_Y);
 }
 template <typename C, int N> __host__ __device__ constexpr size_t fast_smem_x() {
-    return sizeof(C) * (2 * (size_t)N + 6 * (size_t)N * FastTiles<C>::TP_X);
+    return sizeof(C) * (2 * (size_t)N + 6 * (size_t)FastPlan<N>::R1 * fast_x_kstride<C, N>());
 }
+
+// launch bounds: threads per CTA and the CTAs per SM the register allocation must allow
+template <typename C, int N> struct FastLB;
+template <int N> struct FastLB<float2, N> {
+    static constexpr int ROW = 256, COL = 256, XT = 3 * 16 * 8, ROW_MIN = 3, COL_MIN = 3, X_MIN = 2;
+};
+template <int N> struct FastLB<double2, N> {
+    static constexpr int ROW = 128, COL = 128, XT = 3 * 16 * 4, ROW_MIN = 3, COL_MIN = 3, X_MIN = 2;
+};
 
 // ---------------------------------------------------------------------------
 // F1 (row pass): forward z with padding fused into the load.
-// E layout: E[h][k1][row][n2] with row stride (R2 + 1).
+// E layout: E[h][row][k1][n2], k1 stride R2 + 1 (conflict-free transposed reads).
 // ---------------------------------------------------------------------------
 template <typename C, int N, class Pro>
-__global__ void __launch_bounds__(256) kf_fwd_z(OpDev<C> op, Pro pro) {
+__global__ void __launch_bounds__(FastLB<C, N>::ROW, FastLB<C, N>::ROW_MIN) kf_fwd_z(OpDev<C> op, Pro pro) {
     constexpr int R1 = FastPlan<N>::R1, R2 = FastPlan<N>::R2, L = fast_lanes<C, N>(), ROWS = fast_rows<C, N>();
     constexpr int SR = R2 + 1;                 // padded row of E
-    constexpr int HS = R1 * ROWS * SR;         // one half
+    constexpr int HS = R1 * ROWS * SR;         // one half: [ROWS][R1][SR]
     C* tw;
     C* E = fast_smem<C, N>(op.ax[2].tw, tw);
     const int lane = threadIdx.x % L, r = threadIdx.x / L;
@@ -110,7 +123,7 @@ __global__ void __launch_bounds__(256) kf_fwd_z(OpDev<C> op, Pro pro) {
 #pragma unroll
             for (int k1 = 0; k1 < R1; k1++) {
                 const C t = k1 ? cmul(a[k1], tw[2 * n2 * k1]) : a[k1];
-                E[h * HS + (k1 * ROWS + r) * SR + n2] = t;
+                E[h * HS + (r * R1 + k1) * SR + n2] = t;
             }
         }
     }
@@ -121,7 +134,7 @@ __global__ void __launch_bounds__(256) kf_fwd_z(OpDev<C> op, Pro pro) {
 #pragma unroll
         for (int h = 0; h < 2; h++) {
 #pragma unroll
-            for (int n2 = 0; n2 < R2; n2++) X[h][n2] = E[h * HS + (k1 * ROWS + r) * SR + n2];
+            for (int n2 = 0; n2 < R2; n2++) X[h][n2] = E[h * HS + (r * R1 + k1) * SR + n2];
             dft_reg<R2, false>(X[h]);
         }
         C* dst = op.b + ((long long)s * nrows + row) * (2 * N);
@@ -136,10 +149,10 @@ __global__ void __launch_bounds__(256) kf_fwd_z(OpDev<C> op, Pro pro) {
 
 // ---------------------------------------------------------------------------
 // I1 (row pass): inverse z, crop, diagonal term, mask, epilogue.
-// E layout: E[h][n2][row][k1] with row stride (R1 + 1).
+// E layout: E[h][row][n2][k1], n2 stride R1 + 1.
 // ---------------------------------------------------------------------------
 template <typename C, int N, bool CONJ, class Epi>
-__global__ void __launch_bounds__(256) kf_inv_z(OpDev<C> op, const C* __restrict__ xin, Epi epi,
+__global__ void __launch_bounds__(FastLB<C, N>::ROW, FastLB<C, N>::ROW_MIN) kf_inv_z(OpDev<C> op, const C* __restrict__ xin, Epi epi,
                                                 double2* __restrict__ partial) {
     using R = typename real_of<C>::type;
     constexpr int R1 = FastPlan<N>::R1, R2 = FastPlan<N>::R2, L = fast_lanes<C, N>(), ROWS = fast_rows<C, N>();
@@ -169,7 +182,7 @@ __global__ void __launch_bounds__(256) kf_inv_z(OpDev<C> op, const C* __restrict
 #pragma unroll
             for (int n2 = 0; n2 < R2; n2++) {
                 const C t = n2 ? cmulc(X[h][n2], tw[2 * n2 * k1]) : X[h][n2];
-                E[h * HS + (n2 * ROWS + r) * SR + k1] = t;
+                E[h * HS + (r * R2 + n2) * SR + k1] = t;
             }
         }
     }
@@ -183,8 +196,8 @@ __global__ void __launch_bounds__(256) kf_inv_z(OpDev<C> op, const C* __restrict
         C y0[R1], y1[R1];
 #pragma unroll
         for (int k1 = 0; k1 < R1; k1++) {
-            y0[k1] = E[(n2 * ROWS + r) * SR + k1];
-            y1[k1] = E[HS + (n2 * ROWS + r) * SR + k1];
+            y0[k1] = E[(r * R2 + n2) * SR + k1];
+            y1[k1] = E[HS + (r * R2 + n2) * SR + k1];
         }
         dft_reg<R1, true>(y0);
         dft_reg<R1, true>(y1);
@@ -217,7 +230,7 @@ __global__ void __launch_bounds__(256) kf_inv_z(OpDev<C> op, const C* __restrict
 // E layout: E[h][k1][n2][tx].
 // ---------------------------------------------------------------------------
 template <typename C, int N>
-__global__ void __launch_bounds__(256) kf_fwd_y(OpDev<C> op) {
+__global__ void __launch_bounds__(FastLB<C, N>::COL, FastLB<C, N>::COL_MIN) kf_fwd_y(OpDev<C> op) {
     constexpr int R1 = FastPlan<N>::R1, R2 = FastPlan<N>::R2, TP = FastTiles<C>::TP_Y;
     constexpr int HS = N * TP;
     C* tw;
@@ -262,7 +275,7 @@ __global__ void __launch_bounds__(256) kf_fwd_y(OpDev<C> op) {
 
 // I2 (column pass): inverse y, crop.  E layout: E[h][n2][k1][tx].
 template <typename C, int N>
-__global__ void __launch_bounds__(256) kf_inv_y(OpDev<C> op) {
+__global__ void __launch_bounds__(FastLB<C, N>::COL, FastLB<C, N>::COL_MIN) kf_inv_y(OpDev<C> op) {
     constexpr int R1 = FastPlan<N>::R1, R2 = FastPlan<N>::R2, TP = FastTiles<C>::TP_Y;
     constexpr int HS = N * TP;
     C* tw;
@@ -308,16 +321,18 @@ __global__ void __launch_bounds__(256) kf_inv_y(OpDev<C> op) {
 
 // ---------------------------------------------------------------------------
 // F3 (column pass, three components): forward x, spectral multiply, inverse x,
-// crop.  grid (kz tiles of TP, 2ny).  E layout: E[s][h][k1][n2][tx] (forward)
+// crop.  grid (kz tiles of TP, 2ny).  E layout: E[s][h][k1][n2][tx], k1 blocks
+// padded by TP entries (forward)
 // then E[s][h][k1][k2][tx] (spectra) then E[s][h][k1][n2][tx] (inverse).
 // Thread roles: steps A/A' (tx, s, n2); step B / multiply / B' (tx, h, k1).
 // ---------------------------------------------------------------------------
 template <typename C, int N, bool CONJ>
-__global__ void __launch_bounds__(384) kf_x_spectral(OpDev<C> op) {
+__global__ void __launch_bounds__(FastLB<C, N>::XT, FastLB<C, N>::X_MIN) kf_x_spectral(OpDev<C> op) {
     using R = typename real_of<C>::type;
     constexpr int R1 = FastPlan<N>::R1, R2 = FastPlan<N>::R2, TP = FastTiles<C>::TP_X;
     constexpr int L = R1 > R2 ? R1 : R2;
-    constexpr int HS = N * TP, SS = 2 * HS;
+    constexpr int KS = fast_x_kstride<C, N>();  // stride of k1 (R2*TP + TP padding)
+    constexpr int HS = R1 * KS, SS = 2 * HS;
     C* tw;
     C* E = fast_smem<C, N>(op.ax[0].tw, tw);
     const int Lz = 2 * op.nz, Ly = 2 * op.ny;
@@ -344,7 +359,7 @@ __global__ void __launch_bounds__(384) kf_x_spectral(OpDev<C> op) {
                 dft_reg<R1, false>(a);
 #pragma unroll
                 for (int k1 = 0; k1 < R1; k1++)
-                    E[s * SS + h * HS + (k1 * R2 + n2) * TP + tx] = k1 ? cmul(a[k1], tw[2 * n2 * k1]) : a[k1];
+                    E[s * SS + h * HS + k1 * KS + n2 * TP + tx] = k1 ? cmul(a[k1], tw[2 * n2 * k1]) : a[k1];
             }
         }
     }
@@ -355,7 +370,7 @@ __global__ void __launch_bounds__(384) kf_x_spectral(OpDev<C> op) {
         const int h = q / R1, k1 = q % R1;
         if (h < 2 && live) {
             const int md = CONJ ? 1 : 0;
-            C* base = E + h * HS + (k1 * R2) * TP + tx;  // + s*SS + k2*TP
+            C* base = E + h * HS + k1 * KS + tx;  // + s*SS + k2*TP
 #pragma unroll
             for (int s = 0; s < 3; s++) {
                 C X[R2];
@@ -404,8 +419,8 @@ __global__ void __launch_bounds__(384) kf_x_spectral(OpDev<C> op) {
             C y0[R1], y1[R1];
 #pragma unroll
             for (int k1 = 0; k1 < R1; k1++) {
-                y0[k1] = E[s * SS + (k1 * R2 + n2) * TP + tx];
-                y1[k1] = E[s * SS + HS + (k1 * R2 + n2) * TP + tx];
+                y0[k1] = E[s * SS + k1 * KS + n2 * TP + tx];
+                y1[k1] = E[s * SS + HS + k1 * KS + n2 * TP + tx];
             }
             dft_reg<R1, true>(y0);
             dft_reg<R1, true>(y1);

@@ -226,6 +226,14 @@ struct FinBicgBeta {  // d0 = r^T r (v2); beta = 1/v2; err = sqrt(|v2|^2/|vx|^2)
         if (!dfinite(S[S_ERR]) || !dfinite(S[S_BETA])) S[S_NAN] = make_double2(1.0, 0.0);
     }
 };
+// reliable update: rho := b^H r for the replaced residual and the beta of the next step
+struct FinRhoReset {  // d0 = b^H r(true)
+    __device__ void operator()(double2* S, const double2* d) const {
+        S[S_RHO] = d[0];
+        S[S_BETA] = dmul(ddiv(d[0], S[S_RHO1]), ddiv(S[S_ALPHA], S[S_OMEGA]));
+        if (!dfinite(S[S_BETA])) S[S_NAN] = make_double2(1.0, 0.0);
+    }
+};
 // refinement -------------------------------------------------------------------
 struct FinNorm {  // S[slot] = d0 (a squared norm)
     int slot;
@@ -339,6 +347,24 @@ __global__ void k_scale_to(C* __restrict__ y, const double2* __restrict__ x, lon
     const double s = 1.0 / sqrt(S[slot].x);
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
         y[i] = from_d2<C>(make_double2(x[i].x * s, x[i].y * s));
+}
+
+// y32 = float(x64)
+__global__ void k_to_f32(float2* __restrict__ y, const double2* __restrict__ x, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        y[i] = make_float2((float)x[i].x, (float)x[i].y);
+}
+
+// x64 += x32; x32 = 0 (the FP64 solution update of a reliable-update step)
+__global__ void k_fold_correction(double2* __restrict__ x64, float2* __restrict__ x32, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const float2 d = x32[i];
+        double2 v = x64[i];
+        v.x += (double)d.x;
+        v.y += (double)d.y;
+        x64[i] = v;
+        x32[i] = make_float2(0.f, 0.f);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -874,6 +900,106 @@ static int true_residual(vie_ctx* ctx, const double2* b, const double2* x, doubl
     return VIE_OK;
 }
 
+// BiCGSTAB in FP32 with reliable updates in FP64 (mixed precision).
+//
+// The recurrences of BICGSTAB_FFT (CG_Iteration.h:591-748) run on FP32 vectors
+// with the fused FP32 operator; scalars and inner products stay FP64.  When
+// the recursive residual has fallen by `delta` below its largest value since
+// the last update (or below the tolerance), the FP32 correction is folded into
+// the FP64 solution, r = b - A x is recomputed with the FP64 operator, and that
+// true residual replaces the FP32 one (rho and beta follow it).  The Krylov
+// directions p, v are kept, so no subspace is lost as in a restart.  The solve
+// stops only on the FP64 true residual.
+static int solve_bicgstab_mixed(vie_ctx* ctx, const double2* b64, double2* x64, double tol, double delta,
+                                int maxit, int verbose, KrylovResult& res, int& updates, int& mv64) {
+    using C = float2;
+    int rc = VIE_OK;
+    const long long a = ctx->a, n = 3 * a;
+    Operator<float>& op = ctx->op32;
+    C* r = (C*)work_vec(ctx, 8, sizeof(C), &rc);
+    C* p = (C*)work_vec(ctx, 9, sizeof(C), &rc);
+    C* v = (C*)work_vec(ctx, 10, sizeof(C), &rc);
+    C* sv = (C*)work_vec(ctx, 11, sizeof(C), &rc);
+    C* t = (C*)work_vec(ctx, 12, sizeof(C), &rc);
+    C* x32 = (C*)work_vec(ctx, 13, sizeof(C), &rc);
+    C* b32 = (C*)work_vec(ctx, 14, sizeof(C), &rc);
+    double2* r64 = (double2*)work_vec(ctx, 21, sizeof(double2), &rc);
+    if (rc) return rc;
+    cudaStream_t st = ctx->stream;
+    VIE_CUDA_TRY(cudaMemsetAsync(ctx->d_scal, 0, sizeof(double2) * S_COUNT, st), ctx->err);
+    VIE_CUDA_TRY(cudaMemsetAsync(x64, 0, sizeof(double2) * n, st), ctx->err);
+    VIE_CUDA_TRY(cudaMemsetAsync(x32, 0, sizeof(C) * n, st), ctx->err);
+    k_to_f32<<<kVecBlocks, 256, 0, st>>>(b32, b64, n);
+    count_launch();
+    VIE_CUDA_TRY(cudaMemcpyAsync(r, b32, sizeof(C) * n, cudaMemcpyDeviceToDevice, st), ctx->err);
+    {
+        // ||b||^2 from the FP64 right-hand side, rho = b^H r in FP32 data
+        DotArgs<double2, 1> g{{b64}, {b64}, {1}};
+        if ((rc = dots(ctx, g))) return rc;
+        if ((rc = finalize<1>(ctx, kVecBlocks, FinNorm{S_T5}))) return rc;
+        DotArgs<C, 2> g2{{b32, b32}, {b32, r}, {1, 1}};
+        if ((rc = dots(ctx, g2))) return rc;
+        if ((rc = finalize<2>(ctx, kVecBlocks, FinBicgstabInit{}))) return rc;
+        if ((rc = read_scalars(ctx))) return rc;
+    }
+    const double bn2 = ctx->h_scal[S_T5].x;
+    double rmax2 = bn2;
+    const long long nblk = epilogue_blocks(op);
+    for (int m = 0; m < maxit; m++) {
+        if (m == 0) {
+            if ((rc = opmv(ctx, op, ProCopyWrite<C>{r, p, a}, EpiDotB<C>{v, b32, a}, p, false))) return rc;
+        } else {
+            if ((rc = opmv(ctx, op, ProBicgP<C>{r, p, v, ctx->d_scal, a}, EpiDotB<C>{v, b32, a}, p, false))) return rc;
+        }
+        if ((rc = finalize<1>(ctx, nblk, FinAlpha{}))) return rc;
+        if ((rc = opmv(ctx, op, ProBicgS<C>{r, v, sv, ctx->d_scal, a}, EpiDotTS<C>{t, sv, a}, sv, false))) return rc;
+        if ((rc = finalize<2>(ctx, nblk, FinOmega{}))) return rc;
+        k_bicgstab_update<C><<<kVecBlocks, 256, 0, st>>>(x32, p, sv, t, r, b32, n, ctx->d_scal, ctx->d_partial);
+        count_launch();
+        VIE_CUDA_TRY(cudaGetLastError(), ctx->err);
+        if ((rc = finalize<2>(ctx, kVecBlocks, FinBicgstabUpdate{}))) return rc;
+        res.matvecs += 2;
+        res.iterations = m + 1;
+        if ((rc = read_scalars(ctx))) return rc;
+        const double rr = ctx->h_scal[S_RR].x;
+        double err = std::sqrt(rr / bn2);
+        res.err = err;
+        if (ctx->h_scal[S_NAN].x != 0.0 && !(err < tol)) {
+            res.status = VIE_ERR_BREAKDOWN;
+            return ctx->set_error(VIE_ERR_BREAKDOWN, "mixed BiCGSTAB breakdown at step " + std::to_string(m));
+        }
+        if (rr < delta * delta * rmax2 || err < tol) {
+            // reliable update: x += x32 in FP64, r = b - A x in FP64, r32 = float(r)
+            k_fold_correction<<<kVecBlocks, 256, 0, st>>>(x64, x32, n);
+            count_launch();
+            VIE_CUDA_TRY(cudaGetLastError(), ctx->err);
+            double rel;
+            double2 bnv = make_double2(bn2, 0.0);
+            if ((rc = true_residual(ctx, b64, x64, r64, &rel, &bnv))) return rc;
+            updates++;
+            mv64++;
+            err = rel;
+            res.err = rel;
+            if (verbose) printf("CG Error: %lf (true residual)\n", rel);
+            if (rel < tol) {
+                res.steps = m;
+                return VIE_OK;
+            }
+            k_to_f32<<<kVecBlocks, 256, 0, st>>>(r, r64, n);
+            count_launch();
+            DotArgs<C, 1> g{{b32}, {r}, {1}};
+            if ((rc = dots(ctx, g))) return rc;
+            if ((rc = finalize<1>(ctx, kVecBlocks, FinRhoReset{}))) return rc;
+            rmax2 = rel * rel * bn2;
+        } else {
+            rmax2 = std::max(rmax2, rr);
+            if (verbose) printf("CG Error: %lf\n", err);
+        }
+    }
+    res.status = VIE_ERR_MAXIT;
+    return VIE_OK;
+}
+
 int solve_driver(vie_ctx* ctx, const vie_solve_params* prm, vie_solve_info* info) {
     int rc = ensure_scalars(ctx);
     if (rc) return rc;
@@ -911,6 +1037,20 @@ int solve_driver(vie_ctx* ctx, const vie_solve_params* prm, vie_solve_info* info
         out.iterations = res.iterations;
         out.matvecs_fp64 = res.matvecs;
         out.relres = res.err;
+    } else if (prm->precision == VIE_PREC_MIXED && prm->solver == VIE_SOLVER_BICGSTAB) {
+        KrylovResult res;
+        int updates = 0, mv64 = 0;
+        const double delta = prm->inner_tol > 0 ? prm->inner_tol : 0.1;
+        rc = solve_bicgstab_mixed(ctx, b64, ctx->d_x, prm->tol, delta, maxit, prm->verbose, res, updates, mv64);
+        if (rc && rc != VIE_ERR_BREAKDOWN) return rc;
+        status = rc == VIE_ERR_BREAKDOWN ? VIE_ERR_BREAKDOWN : res.status;
+        out.steps = res.steps;
+        out.iterations = res.iterations;
+        out.outer = updates;
+        out.matvecs_fp32 = res.matvecs;
+        out.matvecs_fp64 = mv64;
+        out.relres = res.err;
+        ctx->err.code = VIE_OK;
     } else if (prm->precision == VIE_PREC_MIXED) {
         // FP32 inner Krylov inside FP64 defect correction:
         //   r = b - A x (FP64);  solve A d = r / ||r|| in FP32;  x += ||r|| d (FP64)

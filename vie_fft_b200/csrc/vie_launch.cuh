@@ -18,8 +18,11 @@ inline cudaError_t ensure_smem(const void* kernel, size_t bytes) {
     cudaGetDevice(&dev);
     std::lock_guard<std::mutex> lk(mu);
     size_t& cur = set_bytes[dev & 63][kernel];
-    if (bytes <= cur) return cudaSuccess;
+    if (bytes <= cur && cur > 0) return cudaSuccess;
     cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    // prefer the largest shared-memory carveout so several CTAs of the pencil passes fit per SM
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
     if (e == cudaSuccess) cur = bytes;
     return e;
 }
