@@ -114,6 +114,18 @@ VIE_API int vie_matvec(vie_ctx* ctx, const double* x, double* y, int conj);
    serialised by the caller.  The first call on a device looks up the array's
    device address; make it before any stream capture. */
 VIE_API int vie_matvec_static(vie_ctx* ctx, const double* x, double* y, int conj);
+/* Parts of one operator application, for the reference's block functions:
+   VIE_PART_GREEN  the FFT blocks L_DC_Dq / L_Dq (fft.h:41-127, 224-309)
+   VIE_PART_DIAG   the diagonal terms LXX_DO / LYY_DO / LZZ_DO (fft.h:405-588)
+   VIE_PART_MASK   Current_Reset of the output (fft.h:13-35)
+   vie_matvec is vie_apply with VIE_PART_ALL; X_FFT etc. are GREEN | DIAG. */
+#define VIE_PART_GREEN 1
+#define VIE_PART_DIAG 2
+#define VIE_PART_MASK 4
+#define VIE_PART_ALL 7
+VIE_API int vie_apply(vie_ctx* ctx, const double* x, double* y, int conj, int parts);
+/* Current_Reset (fft.h:13-35): v (a complex, host) *= Flag of component comp (0 x, 1 y, 2 z). */
+VIE_API int vie_reset(vie_ctx* ctx, double* v, int comp);
 /* Same on device buffers of the context's GPU.  precision VIE_PREC_FP64:
    x, y are 3a double2; VIE_PREC_MIXED: 3a float2 (the FP32 operator).
    Runs on the context stream; returns after the launch (no sync). */

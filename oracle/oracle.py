@@ -125,6 +125,9 @@ def ref_lib():
             L.ref_farfield2.argtypes = [_dp, _dp]
             L.ref_nearfield.argtypes = [_dp, _dp, _dp]
             L.ref_set_verbose.argtypes = [ctypes.c_int]
+            L.ref_row.argtypes = [ctypes.c_int, _dp, _dp]
+            L.ref_block.argtypes = [ctypes.c_int] * 4 + [_dp, _dp]
+            L.ref_reset.argtypes = [_dp, ctypes.c_int]
             _ref = L
     return _ref
 
@@ -280,6 +283,25 @@ class Reference:
         a = ctypes.c_double(0)
         self.L.ref_nearfield(ctypes.byref(e), ctypes.byref(m), ctypes.byref(a))
         return e.value, m.value, a.value
+
+    def row(self, which, x):
+        """X/Y/Z_FFT (which 0..2) or their _Conjugate twins (3..5), field from zero."""
+        x = np.ascontiguousarray(x, np.complex128)
+        out = np.zeros(self.g.shape, np.complex128)
+        self.L.ref_row(int(which), _p(x), _p(out))
+        return out
+
+    def block(self, kind, src, fld, conj, x):
+        """L_DC_Dq (kind 0), L_Dq (1) or L??_DO (2) on component src of x after Current_Expansion."""
+        x = np.ascontiguousarray(x, np.complex128)
+        out = np.zeros(self.g.shape, np.complex128)
+        self.L.ref_block(int(kind), int(src), int(fld), int(conj), _p(x), _p(out))
+        return out
+
+    def reset(self, v, flag):
+        v = np.array(v, dtype=np.complex128, order="C", copy=True)
+        self.L.ref_reset(_p(v), int(flag))
+        return v
 
     def set_cross_section(self, cs):
         self.L.ref_set_cross_section(cs)

@@ -288,6 +288,77 @@ int ref_matvec(const double* in, double* out, int conj) {
     return 0;
 }
 
+/* Per-function parity of the operator pieces.  `which`:
+   0..2  X_FFT / Y_FFT / Z_FFT (CG_Iteration.h:131-173) on (in) -> field
+   3..5  the _Conjugate twins (:86-128)
+   Field starts at zero, no Current_Reset (the drivers reset afterwards). */
+int ref_row(int which, const double* in, double* out) {
+    if (!g_inputs_live || !g_current_live) return 1;
+    int Dim[3] = {Nx, Ny, Nz};
+    size_t a = (size_t)Nx * Ny * Nz;
+    MKL_Complex16*** sx = NULL; MKL_Complex16*** sy = NULL; MKL_Complex16*** sz = NULL;
+    MKL_Complex16*** f = NULL; MKL_Complex16*** tmp = NULL;
+    sx = Memory3D(sx, Nx, Ny, Nz); sy = Memory3D(sy, Nx, Ny, Nz); sz = Memory3D(sz, Nx, Ny, Nz);
+    f = Memory3D(f, Nx, Ny, Nz); tmp = Memory3D(tmp, NNx, NNy, NNz);
+    memcpy(sx[0][0], in, a * 16); memcpy(sy[0][0], in + 2 * a, a * 16); memcpy(sz[0][0], in + 4 * a, a * 16);
+    memset(f[0][0], 0, a * 16);
+    switch (which) {
+        case 0: X_FFT(f, sx, sy, sz, tmp, Green_Function, Dim); break;
+        case 1: Y_FFT(f, sx, sy, sz, tmp, Green_Function, Dim); break;
+        case 2: Z_FFT(f, sx, sy, sz, tmp, Green_Function, Dim); break;
+        case 3: X_FFT_Conjugate(f, sx, sy, sz, tmp, Green_Function, Dim); break;
+        case 4: Y_FFT_Conjugate(f, sx, sy, sz, tmp, Green_Function, Dim); break;
+        case 5: Z_FFT_Conjugate(f, sx, sy, sz, tmp, Green_Function, Dim); break;
+        default: return 2;
+    }
+    memcpy(out, f[0][0], a * 16);
+    RMemory3D(sx); RMemory3D(sy); RMemory3D(sz); RMemory3D(f); RMemory3D(tmp);
+    return 0;
+}
+
+/* One block on component `src` of (in) after Current_Expansion (CG_Iteration.h:50-83):
+   kind 0 L_DC_Dq (fld = src), 1 L_Dq, 2 L??_DO of src; conj selects the
+   _Conjugate twin.  Field starts at zero. */
+int ref_block(int kind, int src, int fld, int conj, const double* in, double* out) {
+    if (!g_inputs_live || !g_current_live) return 1;
+    int Dim[3] = {Nx, Ny, Nz};
+    size_t a = (size_t)Nx * Ny * Nz;
+    MKL_Complex16*** J = NULL; MKL_Complex16*** f = NULL; MKL_Complex16*** tmp = NULL;
+    J = Memory3D(J, Nx, Ny, Nz); f = Memory3D(f, Nx, Ny, Nz); tmp = Memory3D(tmp, NNx, NNy, NNz);
+    memcpy(J[0][0], in + 2 * a * src, a * 16);
+    memset(f[0][0], 0, a * 16);
+    Current_Expansion(tmp, J, src, Dim);
+    const double d[3] = {delta_x, delta_y, delta_z};
+    if (kind == 0) {
+        if (conj) L_DC_Dq_Conjugate(f, tmp, Green_Function, d[src], src, Dim);
+        else L_DC_Dq(f, tmp, Green_Function, d[src], src, Dim);
+    } else if (kind == 1) {
+        if (conj) L_Dq_Conjugate(f, tmp, Green_Function, src, fld, d[fld], Dim);
+        else L_Dq(f, tmp, Green_Function, src, fld, d[src], Dim);
+    } else {
+        if (src == 0) { if (conj) LXX_DO_Conjugate(f, tmp, Dim); else LXX_DO(f, tmp, Dim); }
+        if (src == 1) { if (conj) LYY_DO_Conjugate(f, tmp, Dim); else LYY_DO(f, tmp, Dim); }
+        if (src == 2) { if (conj) LZZ_DO_Conjugate(f, tmp, Dim); else LZZ_DO(f, tmp, Dim); }
+    }
+    memcpy(out, f[0][0], a * 16);
+    RMemory3D(J); RMemory3D(f); RMemory3D(tmp);
+    return 0;
+}
+
+/* Current_Reset (fft.h:13-35) on a copy. */
+int ref_reset(double* v, int flag) {
+    if (!g_inputs_live) return 1;
+    int Dim[3] = {Nx, Ny, Nz};
+    size_t a = (size_t)Nx * Ny * Nz;
+    MKL_Complex16*** J = NULL;
+    J = Memory3D(J, Nx, Ny, Nz);
+    memcpy(J[0][0], v, a * 16);
+    Current_Reset(J, flag, Dim);
+    memcpy(v, J[0][0], a * 16);
+    RMemory3D(J);
+    return 0;
+}
+
 /* One self-term block L_DC_Dq (fft.h:41-127) on a pre-expanded (2N)^3 array,
    for per-function timing of the reference (the unit of one matvec is nine of
    these blocks plus cheap O(N^3) work). */

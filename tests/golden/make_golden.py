@@ -15,6 +15,12 @@ Fixtures
   c1_sphere.npz      the 32^3 silver-sphere BiCGSTAB solve to 1e-6: step
                      count, solution on the flagged edges, FarField1 and
                      NearField outputs
+  dropin_blocks.npz  X/Y/Z_FFT rows, L_DC_Dq, L_Dq, L??_DO (and conjugate
+                     twins) and Current_Reset on small seeded cases
+  dropin_program.npz the reference's unchanged main program (CG_FFT_VIE.cpp,
+                     41 wavelengths) on the synthetic material tables of
+                     program_tables(): its Ene_Metal, Ene_Active, Grid and
+                     RCS outputs and the step count of each solve
 """
 from __future__ import annotations
 
@@ -109,10 +115,91 @@ def make_c1():
                         forward_rcs=fwd, ext_over_cs=ext, metal_abs_over_cs=metal)
 
 
+def make_dropin_blocks():
+    out = {}
+    for idx in (0, 1, 3):
+        shape, d, k0, ang, mat, flags, x = small_inputs(idx)
+        g = O.Grid(*shape, *d, k0)
+        R = O.Reference(g, EPS_TABLE, *ang)
+        R.set_geometry(mat, flags)
+        R.green()
+        for which in range(6):
+            out[f"row{idx}_{which}"] = R.row(which, x)
+        for conj in (0, 1):
+            for src in range(3):
+                out[f"blk{idx}_0_{src}_{src}_{conj}"] = R.block(0, src, src, conj, x)
+                out[f"blk{idx}_2_{src}_{src}_{conj}"] = R.block(2, src, src, conj, x)
+                for fld in range(3):
+                    if fld != src:
+                        out[f"blk{idx}_1_{src}_{fld}_{conj}"] = R.block(1, src, fld, conj, x)
+        for flag in range(3):
+            out[f"reset{idx}_{flag}"] = R.reset(x[flag], flag)
+        R.release()
+    np.savez_compressed(os.path.join(OUT, "dropin_blocks.npz"), **out)
+
+
+def program_tables():
+    """Synthetic permittivity tables (41 rows, 400-800 nm, reference sign) for
+    the files the main program reads: PEDOT_epr.txt, Au_epr.txt, P3HT_PCBM_epr.txt."""
+    lam = 400.0 + 10.0 * np.arange(41)
+    t = (lam - 400.0) / 400.0
+    pedot = np.stack([2.4 + 0.1 * t, -0.05 - 0.02 * t], 1)
+    metal = np.stack([-1.0 - 4.0 * t, -3.0 + 0.5 * t], 1)
+    p3ht = np.stack([3.8 - 0.4 * t, -0.6 + 0.3 * t], 1)
+    return {"PEDOT_epr.txt": pedot, "Au_epr.txt": metal, "P3HT_PCBM_epr.txt": p3ht}
+
+
+def write_program_tree(root):
+    """data/ with the tables, result/ for the outputs, run/ as the working directory."""
+    for sub in ("data", "result", "run"):
+        os.makedirs(os.path.join(root, sub), exist_ok=True)
+    for name, tab in program_tables().items():
+        with open(os.path.join(root, "data", name), "w") as f:
+            for re_, im_ in tab:
+                f.write(f" {re_:.16e}\t {im_:.16e}\n")
+
+
+def read_program_results(root):
+    res = os.path.join(root, "result")
+    metal = np.array([np.loadtxt(os.path.join(res, f"Ene_Metal{m}.txt")) for m in range(41)])
+    active = np.array([np.loadtxt(os.path.join(res, f"Ene_Active{m}.txt")) for m in range(41)])
+    grid = np.array([np.loadtxt(os.path.join(res, f"Grid{m}.txt")) for m in range(41)])
+    rcs = np.array([np.loadtxt(os.path.join(res, f"RCS{m}.txt")) for m in range(41)])
+    return {"metal": metal, "active": active, "grid": grid, "rcs": rcs}
+
+
+def program_steps(stdout):
+    """Step count of every solve, from the drivers' "Steps: m" lines."""
+    return [int(line.split(":")[1]) for line in stdout.splitlines() if line.startswith("Steps:")]
+
+
+def make_dropin_program():
+    import subprocess
+    import tempfile
+    exe = os.path.join(ROOT, "oracle", "_ref", "vie_fft_ref_main")
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref-main"], check=True)
+    with tempfile.TemporaryDirectory() as tmp:
+        write_program_tree(tmp)
+        run = subprocess.run([exe], cwd=os.path.join(tmp, "run"), check=True, stdout=subprocess.PIPE,
+                             encoding="latin-1")
+        out = read_program_results(tmp)
+    out["steps"] = np.array(program_steps(run.stdout))
+    np.savez_compressed(os.path.join(OUT, "dropin_program.npz"), **out)
+
+
 if __name__ == "__main__":
-    make_small_ops()
-    make_small_solves()
-    make_c1()
+    import sys as _sys
+    which = _sys.argv[1:] or ["ops", "solves", "c1", "blocks", "program"]
+    if "ops" in which:
+        make_small_ops()
+    if "solves" in which:
+        make_small_solves()
+    if "c1" in which:
+        make_c1()
+    if "blocks" in which:
+        make_dropin_blocks()
+    if "program" in which:
+        make_dropin_program()
     for f in sorted(os.listdir(OUT)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(OUT, f)))

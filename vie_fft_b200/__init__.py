@@ -33,6 +33,7 @@ VIE_ERR_TIMEOUT = 8
 VIE_ERR_NODEVICE = 9
 
 SOLVERS = {"cg": 1, "bicg": 2, "bicgstab": 3, "cors": 4, "bicorstab": 5}
+PART_GREEN, PART_DIAG, PART_MASK, PART_ALL = 1, 2, 4, 7
 PREC_FP64 = 0
 PREC_MIXED = 1
 
@@ -96,6 +97,8 @@ def lib():
         L.vie_incident.argtypes = [_vp, ctypes.c_double, ctypes.c_double, ctypes.c_double, _dp]
         L.vie_set_rhs.argtypes = [_vp, _dp]
         L.vie_matvec.argtypes = [_vp, _dp, _dp, ctypes.c_int]
+        L.vie_apply.argtypes = [_vp, _dp, _dp, ctypes.c_int, ctypes.c_int]
+        L.vie_reset.argtypes = [_vp, _dp, ctypes.c_int]
         L.vie_matvec_dev.argtypes = [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int]
         L.vie_solve.argtypes = [_vp, P(VieSolveParams), _dp, P(VieSolveInfo)]
         L.vie_get_solution.argtypes = [_vp, _dp]
@@ -209,6 +212,19 @@ class Context:
         y = np.zeros_like(x)
         self._check(self._L.vie_matvec(self._h, _p(x), _p(y), int(bool(conj))))
         return y
+
+    def apply(self, x, conj=False, parts=7):
+        """Selected parts of the operator (PART_GREEN | PART_DIAG | PART_MASK)."""
+        x = _c128(x, (3,) + self.shape)
+        y = np.zeros_like(x)
+        self._check(self._L.vie_apply(self._h, _p(x), _p(y), int(bool(conj)), int(parts)))
+        return y
+
+    def reset(self, v, comp):
+        """Current_Reset of one component (in place on a copy, returned)."""
+        v = np.array(v, dtype=np.complex128, order="C", copy=True)
+        self._check(self._L.vie_reset(self._h, _p(v), int(comp)))
+        return v
 
     def matvec_dev(self, x_ptr: int, y_ptr: int, conj=False, precision=PREC_FP64):
         """Device-pointer operator application (e.g. torch tensor data_ptr())."""

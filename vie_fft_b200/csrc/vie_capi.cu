@@ -14,6 +14,7 @@ int green_expand(vie_ctx* ctx, double2* d_out);
 int incident_compute(vie_ctx* ctx, double theta, double phi, double psi, double2* d_e);
 int solve_driver(vie_ctx* ctx, const vie_solve_params* prm, vie_solve_info* info);
 int residual_driver(vie_ctx* ctx, double* relres);
+void mask_component(double2* v, const unsigned char* flags, long long a, int comp, cudaStream_t st);
 }  // namespace vie
 
 using namespace vie;
@@ -266,8 +267,10 @@ int vie_matvec_dev(vie_ctx* ctx, const void* x, void* y, int conj, int precision
     return ctx->set_error(VIE_ERR_ARG, "precision must be VIE_PREC_FP64 or VIE_PREC_MIXED");
 }
 
-int vie_matvec(vie_ctx* ctx, const double* x, double* y, int conj) {
-    if (check_ctx(ctx) || !x || !y) return VIE_ERR_ARG;
+int vie_matvec(vie_ctx* ctx, const double* x, double* y, int conj) { return vie_apply(ctx, x, y, conj, VIE_PART_ALL); }
+
+int vie_apply(vie_ctx* ctx, const double* x, double* y, int conj, int parts) {
+    if (check_ctx(ctx) || !x || !y || (parts & ~VIE_PART_ALL)) return VIE_ERR_ARG;
     int rc = ready_for_operator(ctx);
     if (rc) return rc;
     cudaSetDevice(ctx->device);
@@ -280,7 +283,9 @@ int vie_matvec(vie_ctx* ctx, const double* x, double* y, int conj) {
     }
     cudaError_t e = cudaMemcpyAsync(dx, x, bytes, cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess) {
-        rc = ctx->op64.apply(dx, dy, conj != 0, ctx->stream, ctx->err);
+        vie::Operator<double> op = ctx->op64;  // same tables and scratch, selected parts
+        op.dev.parts = parts;
+        rc = op.apply(dx, dy, conj != 0, ctx->stream, ctx->err);
         if (!rc) {
             e = cudaMemcpyAsync(y, dy, bytes, cudaMemcpyDeviceToHost, ctx->stream);
             if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
@@ -290,6 +295,25 @@ int vie_matvec(vie_ctx* ctx, const double* x, double* y, int conj) {
     cudaFree(dx);
     cudaFree(dy);
     return rc;
+}
+
+int vie_reset(vie_ctx* ctx, double* v, int comp) {
+    if (check_ctx(ctx) || !v || comp < 0 || comp > 2) return VIE_ERR_ARG;
+    if (!ctx->have_flags) return ctx->set_error(VIE_ERR_STATE, "edge flags not set (vie_set_flags)");
+    cudaSetDevice(ctx->device);
+    const size_t bytes = sizeof(double2) * (size_t)ctx->a;
+    double2* d = nullptr;
+    CTX_CUDA(cudaMalloc(&d, bytes));
+    cudaError_t e = cudaMemcpyAsync(d, v, bytes, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) {
+        mask_component(d, ctx->d_flags, ctx->a, comp, ctx->stream);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(v, d, bytes, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cudaFree(d);
+    if (e != cudaSuccess) return ctx->set_error(VIE_ERR_CUDA, cudaGetErrorString(e));
+    return VIE_OK;
 }
 
 int vie_solve(vie_ctx* ctx, const vie_solve_params* p, double* x, vie_solve_info* info) {

@@ -210,9 +210,9 @@ __global__ void __launch_bounds__(FastLB<C, N>::ROW, FastLB<C, N>::ROW_MIN) kf_i
             const int n = n2 + R2 * n1;
             const long long idx = row * N + n;
             C y = czero<C>();
-            if ((op.flags[idx] >> s) & 1) {
-                y = cadd(y0[n1], cmulc(y1[n1], tw[n]));
-                if (vrow && (s != 2 || n < N - 1)) {
+            if (!(op.parts & 4) || ((op.flags[idx] >> s) & 1)) {
+                if (op.parts & 1) y = cadd(y0[n1], cmulc(y1[n1], tw[n]));
+                if ((op.parts & 2) && vrow && (s != 2 || n < N - 1)) {
                     const C ws = cadd(op.w[idx + sstep], op.w[idx]);
                     C coef = mkc(-dc * ws.y, dc * ws.x);
                     if (CONJ) coef = cconj(coef);

@@ -1162,4 +1162,16 @@ int residual_driver(vie_ctx* ctx, double* relres) {
     return true_residual(ctx, b64, ctx->d_x, r64, relres, &bn2);
 }
 
+// v *= Flag of component comp (Current_Reset, fft.h:13-35)
+__global__ void k_mask_component(double2* __restrict__ v, const unsigned char* __restrict__ flags, long long a,
+                                 int comp) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < a; i += (long long)gridDim.x * blockDim.x)
+        if (!((flags[i] >> comp) & 1)) v[i] = make_double2(0.0, 0.0);
+}
+
+void mask_component(double2* v, const unsigned char* flags, long long a, int comp, cudaStream_t st) {
+    k_mask_component<<<kVecBlocks, 256, 0, st>>>(v, flags, a, comp);
+    count_launch();
+}
+
 }  // namespace vie

@@ -81,6 +81,7 @@ int Operator<T>::init(int nx, int ny, int nz, const double d[3], double k0, cons
     o = OpDev<C>{};
     o.nx = nx; o.ny = ny; o.nz = nz;
     o.a = (long long)nx * ny * nz;
+    o.parts = VIE_PART_ALL;
     const bool dbl = sizeof(T) == 8;
     o.tz = fit_tile<C>(tiles.tz > 0 ? tiles.tz : (dbl ? 8 : 16), nz, 2, 1);
     o.tc = fit_tile<C>(tiles.tc > 0 ? tiles.tc : (dbl ? 8 : 16), ny, 2, 0);

@@ -51,6 +51,7 @@ template <typename C> struct OpDev {
     const C* w;                // per voxel 1/(eps-1)
     const unsigned char* flags;  // bit0 Flag_X, bit1 Flag_Y, bit2 Flag_Z
     int fast[3];               // axis uses the register four-step kernels (half-natural slots)
+    int parts;                 // VIE_PART_* bits: Green blocks, diagonal term, edge mask
     typename real_of<C>::type kappa[3];   // k0^2 delta_f
     typename real_of<C>::type dcoef[3];   // -delta_f Z0 / (2 k0)
     C* b;                      // 3 * nx*ny*2nz scratch
@@ -296,11 +297,11 @@ __global__ void __launch_bounds__(kThreads) k_inv_z(OpDev<C> op, const C* __rest
         if (row >= nrows) continue;
         const long long idx = row * N + n;
         C y = czero<C>();
-        if ((op.flags[idx] >> s) & 1) {
-            y = cadd(buf[n * TP + t], cmulc(buf[fs + n * TP + t], tw[n]));
+        if (!(op.parts & 4) || ((op.flags[idx] >> s) & 1)) {
+            if (op.parts & 1) y = cadd(buf[n * TP + t], cmulc(buf[fs + n * TP + t], tw[n]));
             const int i = (int)(row / op.ny), j = (int)(row - (long long)i * op.ny);
             const bool valid = (s != 0 || i < op.nx - 1) && (s != 1 || j < op.ny - 1) && (s != 2 || n < N - 1);
-            if (valid) {
+            if ((op.parts & 2) && valid) {
                 // -i delta Z0/(2 k0) (w_a + w_b) J   (fft.h:419-433); conjugate twin :455-469
                 const C ws = cadd(op.w[idx + sstep], op.w[idx]);
                 C coef = mkc(-dc * ws.y, dc * ws.x);  // i * dc * ws with dc = -delta Z0/(2 k0)
