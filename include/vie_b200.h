@@ -154,6 +154,8 @@ typedef struct {
     double relres;      /* the solver's own residual estimate at exit */
     double true_relres; /* ||b - A x|| / ||b|| in FP64 at exit (-1 when not evaluated) */
     double seconds;     /* device time of the solve */
+    int graph_loops;    /* iteration loops of the solve that ran as one CUDA graph launch (a device-side
+                           WHILE loop over the captured iteration body); 0: iterated from the host */
 } vie_solve_info;
 
 /* Solve A x = b for the current right-hand side from x0 = 0.  Replaces

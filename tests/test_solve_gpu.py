@@ -148,3 +148,25 @@ def test_iteration_cap_and_errors():
         with pytest.raises(V.VieError) as e:
             c.solve("bicgstab", tol=1e-6)
         assert e.value.status == V.VIE_ERR_STATE
+
+
+@pytest.mark.parametrize("solver,precision", [("bicgstab", V.PREC_FP64), ("cors", V.PREC_FP64), ("cg", V.PREC_FP64),
+                                              ("bicg", V.PREC_FP64), ("bicorstab", V.PREC_FP64),
+                                              ("bicgstab", V.PREC_MIXED), ("cors", V.PREC_MIXED)])
+def test_graph_loop_matches_host_loop(solver, precision, monkeypatch):
+    """The iteration captured once and looped on the device (conditional WHILE
+    node, reliable updates under an IF node) computes exactly what the same
+    kernels launched from a host loop compute."""
+    w = MG.solve_case()
+    tol = 1e-8
+    with ctx_for(w) as c:
+        rg = c.solve(solver, tol=tol, precision=precision)
+    monkeypatch.setenv("VIE_GRAPH", "0")
+    with ctx_for(w) as c:
+        rh = c.solve(solver, tol=tol, precision=precision)
+    assert rg.info["graph_loops"] >= 1 and rh.info["graph_loops"] == 0
+    if precision == V.PREC_FP64 or solver == "bicgstab":
+        assert rg.info["graph_loops"] == 1
+    for k in ("steps", "iterations", "outer", "matvecs_fp32", "matvecs_fp64"):
+        assert rg.info[k] == rh.info[k], k
+    np.testing.assert_array_equal(rg.x, rh.x)

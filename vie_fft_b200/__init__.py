@@ -61,7 +61,7 @@ class VieSolveParams(ctypes.Structure):
 class VieSolveInfo(ctypes.Structure):
     _fields_ = [("steps", ctypes.c_int), ("iterations", ctypes.c_int), ("outer", ctypes.c_int),
                 ("matvecs_fp64", ctypes.c_int), ("matvecs_fp32", ctypes.c_int), ("relres", ctypes.c_double),
-                ("true_relres", ctypes.c_double), ("seconds", ctypes.c_double)]
+                ("true_relres", ctypes.c_double), ("seconds", ctypes.c_double), ("graph_loops", ctypes.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

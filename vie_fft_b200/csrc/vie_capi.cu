@@ -121,6 +121,7 @@ int vie_create(const vie_grid* g, vie_ctx** out) {
     cudaMemset(ctx->d_flags, 0, (size_t)ctx->a);
     cudaMemset(ctx->d_x, 0, sizeof(double2) * 3 * (size_t)ctx->a);
     ctx->w_host.assign(2 * (size_t)ctx->a, 0.0);
+    if (const char* gv = std::getenv("VIE_GRAPH")) ctx->use_graphs = std::atoi(gv) != 0;
     *out = ctx;
     return VIE_OK;
 }
@@ -140,6 +141,10 @@ void vie_destroy(vie_ctx* ctx) {
     if (ctx->d_scal) cudaFree(ctx->d_scal);
     if (ctx->d_partial) cudaFree(ctx->d_partial);
     if (ctx->h_scal) cudaFreeHost(ctx->h_scal);
+    if (ctx->d_ctl) cudaFree(ctx->d_ctl);
+    if (ctx->h_ctl) cudaFreeHost(ctx->h_ctl);
+    if (ctx->d_hist) cudaFree(ctx->d_hist);
+    if (ctx->stream_aux) cudaStreamDestroy(ctx->stream_aux);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }

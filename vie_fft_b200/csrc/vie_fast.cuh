@@ -91,6 +91,7 @@ template <int N> struct FastLB<double2, N> {
 // ---------------------------------------------------------------------------
 template <typename C, int N, class Pro>
 __global__ void __launch_bounds__(FastLB<C, N>::ROW, FastLB<C, N>::ROW_MIN) kf_fwd_z(OpDev<C> op, Pro pro) {
+    if (gate_closed(op.gate)) return;
     constexpr int R1 = FastPlan<N>::R1, R2 = FastPlan<N>::R2, L = fast_lanes<C, N>(), ROWS = fast_rows<C, N>();
     constexpr int SR = R2 + 1;                 // padded row of E
     constexpr int HS = R1 * ROWS * SR;         // one half: [ROWS][R1][SR]
@@ -154,6 +155,7 @@ __global__ void __launch_bounds__(FastLB<C, N>::ROW, FastLB<C, N>::ROW_MIN) kf_f
 template <typename C, int N, bool CONJ, class Epi>
 __global__ void __launch_bounds__(FastLB<C, N>::ROW, FastLB<C, N>::ROW_MIN) kf_inv_z(OpDev<C> op, const C* __restrict__ xin, Epi epi,
                                                 double2* __restrict__ partial) {
+    if (gate_closed(op.gate)) return;
     using R = typename real_of<C>::type;
     constexpr int R1 = FastPlan<N>::R1, R2 = FastPlan<N>::R2, L = fast_lanes<C, N>(), ROWS = fast_rows<C, N>();
     constexpr int SR = R1 + 1;
@@ -231,6 +233,7 @@ __global__ void __launch_bounds__(FastLB<C, N>::ROW, FastLB<C, N>::ROW_MIN) kf_i
 // ---------------------------------------------------------------------------
 template <typename C, int N>
 __global__ void __launch_bounds__(FastLB<C, N>::COL, FastLB<C, N>::COL_MIN) kf_fwd_y(OpDev<C> op) {
+    if (gate_closed(op.gate)) return;
     constexpr int R1 = FastPlan<N>::R1, R2 = FastPlan<N>::R2, TP = FastTiles<C>::TP_Y;
     constexpr int HS = N * TP;
     C* tw;
@@ -276,6 +279,7 @@ __global__ void __launch_bounds__(FastLB<C, N>::COL, FastLB<C, N>::COL_MIN) kf_f
 // I2 (column pass): inverse y, crop.  E layout: E[h][n2][k1][tx].
 template <typename C, int N>
 __global__ void __launch_bounds__(FastLB<C, N>::COL, FastLB<C, N>::COL_MIN) kf_inv_y(OpDev<C> op) {
+    if (gate_closed(op.gate)) return;
     constexpr int R1 = FastPlan<N>::R1, R2 = FastPlan<N>::R2, TP = FastTiles<C>::TP_Y;
     constexpr int HS = N * TP;
     C* tw;
@@ -328,6 +332,7 @@ __global__ void __launch_bounds__(FastLB<C, N>::COL, FastLB<C, N>::COL_MIN) kf_i
 // ---------------------------------------------------------------------------
 template <typename C, int N, bool CONJ>
 __global__ void __launch_bounds__(FastLB<C, N>::XT, FastLB<C, N>::X_MIN) kf_x_spectral(OpDev<C> op) {
+    if (gate_closed(op.gate)) return;
     using R = typename real_of<C>::type;
     constexpr int R1 = FastPlan<N>::R1, R2 = FastPlan<N>::R2, TP = FastTiles<C>::TP_X;
     constexpr int L = R1 > R2 ? R1 : R2;

@@ -80,6 +80,28 @@ enum ScalarSlot {
     S_T0, S_T1, S_T2, S_T3, S_T4, S_T5, S_DONE, S_NAN, S_COUNT
 };
 
+// Device-resident control block of one iterative solve.  The decision at the
+// end of every iteration (converged, breakdown, cap, reliable update) is taken
+// on the device and written to `state`; the kernels of the next iteration are
+// gated on it (Gate), and a captured iteration graph loops while the state is
+// not terminal.
+enum KrylovState { KS_RUN = 0, KS_UPDATE = 1, KS_DONE = 2, KS_BREAKDOWN = 3, KS_MAXIT = 4, KS_RESET = 5 };
+struct KCtl {
+    int state;
+    int iter;      // iterations completed
+    int maxit;
+    int steps;     // step index of convergence (the reference's "Steps")
+    int updates;   // reliable updates
+    int loops;     // executions of the iteration body
+    int hist_cap;  // entries of the history array
+    int pad;
+    double thr;    // threshold on the solver's error measure
+    double delta;  // reliable-update trigger (mixed BiCGSTAB)
+    double rmax2;  // largest ||r||^2 since the last reliable update
+    double bn2;    // FP64 ||b||^2 (mixed BiCGSTAB)
+    double last;   // last error (true residual after an update)
+};
+
 }  // namespace vie
 
 // The opaque context of the C ABI.
@@ -115,6 +137,16 @@ struct vie_ctx {
     double2* d_partial = nullptr;         // reduction partials
     size_t partial_cap = 0;               // entries
     double2* h_scal = nullptr;            // pinned mirror
+    vie::KCtl* d_ctl = nullptr;           // solve control block (device)
+    vie::KCtl* h_ctl = nullptr;           // pinned mirror
+    double2* d_hist = nullptr;            // per iteration: (error, true residual of a reliable update or -1)
+    int hist_cap = 0;
+    vie::Gate gate{nullptr, 0};           // gate applied to launches while an iteration body is enqueued
+    int use_graphs = 1;                   // capture the iteration body in a CUDA graph with a device-side loop
+    long long graph_launches = 0;         // solve loops run as one graph launch
+    int capturing = 0;                    // an iteration body is being captured
+    cudaStream_t stream_aux = nullptr;    // capture stream of conditional (IF) bodies
+    cudaStream_t stream_parent = nullptr; // ctx->stream while an IF body is captured on stream_aux
 
     int set_error(int code, const std::string& m) {
         err.code = code;

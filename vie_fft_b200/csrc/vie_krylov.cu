@@ -4,8 +4,13 @@
 // complex and are produced by one-block finalize kernels from per-block
 // partial sums (fixed summation order, so runs are deterministic).  Dot
 // products always accumulate in FP64, also when the vectors are FP32.  The
-// host only reads the error estimate once per iteration to decide whether to
-// stop, like the reference's printf/break (CG_Iteration.h:733-747).
+// stop decision of every iteration (the reference's printf/break,
+// CG_Iteration.h:733-747) is also taken on the device, into a control block
+// (KCtl); every kernel of an iteration is gated on the control state, so the
+// iteration body is captured once into a CUDA graph whose conditional WHILE
+// node repeats it until the state is terminal: one graph launch per solve, no
+// host round trip per iteration.  The per-iteration errors are kept in a
+// device history and printed after the solve.
 //
 // BiCGSTAB fuses its vector updates into the operator passes:
 //   p = r + beta (p - omega v)    in the first pass of A p  (CG_Iteration.h:611-633)
@@ -16,6 +21,9 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <initializer_list>
+#include <string>
+#include <vector>
 
 #include "vie_launch.cuh"
 
@@ -57,7 +65,8 @@ template <typename C> __device__ __forceinline__ void acc_dotu(double2& acc, C u
 // ---------------------------------------------------------------------------
 template <int K, class Fin>
 __global__ void __launch_bounds__(256) k_finalize(const double2* __restrict__ partial, long long nblk, double2* S,
-                                                  Fin fin) {
+                                                  Fin fin, Gate gate) {
+    if (gate_closed(gate)) return;
     __shared__ double2 red[K][256];
     for (int k = 0; k < K; k++) {
         double rx = 0, ry = 0;
@@ -129,10 +138,10 @@ struct FinBicgstabUpdate {  // d0 = r^H r, d1 = b^H r(new)
 };
 // CORS -----------------------------------------------------------------------
 struct FinCorsRho {  // d0 = b^H A r
-    int first;
+    const KCtl* ctl;
     __device__ void operator()(double2* S, const double2* d) const {
         S[S_RHO] = d[0];
-        if (!first) {
+        if (ctl->iter > 0) {
             const double2 beta = ddiv(d[0], S[S_RHO1]);  // :874-878
             S[S_BETA] = beta;
             S[S_T0] = dmul(beta, beta);
@@ -158,10 +167,10 @@ struct FinErr {  // d0 = r^H r; err = sqrt(rr / bnrm2); rho_1 = rho
 };
 // BiCORSTAB ------------------------------------------------------------------
 struct FinBicorRho {  // d0 = b^H A r
-    int first;
+    const KCtl* ctl;
     __device__ void operator()(double2* S, const double2* d) const {
         S[S_RHO] = d[0];
-        if (!first) {
+        if (ctl->iter > 0) {
             S[S_BETA] = dmul(ddiv(d[0], S[S_RHO1]), ddiv(S[S_ALPHA], S[S_OMEGA]));  // :1167-1173
             S[S_T2] = dmul(S[S_BETA], S[S_OMEGA]);  // beta * omega of the previous step
         }
@@ -239,6 +248,111 @@ struct FinNorm {  // S[slot] = d0 (a squared norm)
     int slot;
     __device__ void operator()(double2* S, const double2* d) const { S[slot] = d[0]; }
 };
+struct FinNone {  // decision only (the scalars are already in place)
+    __device__ void operator()(double2*, const double2*) const {}
+};
+struct FinCtlBn2 {  // FP64 ||b||^2 of the mixed solve into the control block (also the first residual maximum)
+    KCtl* ctl;
+    __device__ void operator()(double2* S, const double2* d) const {
+        ctl->bn2 = d[0].x;
+        ctl->rmax2 = d[0].x;
+    }
+};
+
+// stop decisions ------------------------------------------------------------------
+// a finalize step followed by a decision on the control block
+template <class F, class D> struct FinThen {
+    F f;
+    D dec;
+    __device__ void operator()(double2* S, const double2* d) const {
+        f(S, d);
+        dec(S);
+    }
+};
+template <class F, class D> static FinThen<F, D> then(F f, D dec) { return FinThen<F, D>{f, dec}; }
+
+// the drivers' rule: stop when err < CG_THR (CG_Iteration.h:323-331, 497-505,
+// 733-747, 1022-1035, 1315-1327); a non-finite scalar without convergence is a
+// breakdown; the iteration cap ends the solve
+struct DecideErr {
+    KCtl* ctl;
+    double2* hist;
+    __device__ void operator()(double2* S) const {
+        const double err = S[S_ERR].x;
+        const int m = ctl->iter;
+        if (m < ctl->hist_cap) hist[m] = make_double2(err, -1.0);
+        ctl->iter = m + 1;
+        ctl->last = err;
+        if (err < ctl->thr) {
+            ctl->state = KS_DONE;
+            ctl->steps = m;
+        } else if (S[S_NAN].x != 0.0) {
+            ctl->state = KS_BREAKDOWN;
+        } else if (m + 1 >= ctl->maxit) {
+            ctl->state = KS_MAXIT;
+        }
+    }
+};
+// mixed BiCGSTAB after the FP32 step: request a reliable update when the
+// recursive residual fell by delta below its running maximum, or below the
+// tolerance
+struct DecideReliable {
+    KCtl* ctl;
+    double2* hist;
+    __device__ void operator()(double2* S) const {
+        const double err = S[S_ERR].x, rr = S[S_RR].x;
+        const int m = ctl->iter;
+        if (m < ctl->hist_cap) hist[m] = make_double2(err, -1.0);
+        ctl->iter = m + 1;
+        ctl->last = err;
+        if (S[S_NAN].x != 0.0 && !(err < ctl->thr)) {
+            ctl->state = KS_BREAKDOWN;
+        } else if (rr < ctl->delta * ctl->delta * ctl->rmax2 || err < ctl->thr) {
+            ctl->state = KS_UPDATE;
+        } else {
+            ctl->rmax2 = fmax(ctl->rmax2, rr);
+            if (m + 1 >= ctl->maxit) ctl->state = KS_MAXIT;
+        }
+    }
+};
+// after r = b - A x in FP64 (S_T5 = ||r||^2): stop on the true residual, else
+// replace the FP32 residual by it
+struct DecideTrue {
+    KCtl* ctl;
+    double2* hist;
+    __device__ void operator()(double2* S) const {
+        const double rel = sqrt(S[S_T5].x / ctl->bn2);
+        const int m = ctl->iter - 1;
+        if (m >= 0 && m < ctl->hist_cap) hist[m].y = rel;
+        ctl->updates++;
+        ctl->last = rel;
+        if (rel < ctl->thr) {
+            ctl->state = KS_DONE;
+            ctl->steps = m;
+        } else if (ctl->iter >= ctl->maxit) {
+            ctl->state = KS_MAXIT;
+        } else {
+            ctl->state = KS_RESET;
+            ctl->rmax2 = rel * rel * ctl->bn2;
+        }
+    }
+};
+struct DecideResume {  // residual replaced: iterate again
+    KCtl* ctl;
+    __device__ void operator()(double2*) const { ctl->state = KS_RUN; }
+};
+
+// end of one iteration body: count it and set the WHILE condition of the graph
+__global__ void k_loop_cond(KCtl* ctl, cudaGraphConditionalHandle h) {
+    ctl->loops++;
+    const int s = ctl->state;
+    cudaGraphSetConditional(h, (s == KS_RUN || s == KS_UPDATE || s == KS_RESET) ? 1u : 0u);
+}
+__global__ void k_loop_count(KCtl* ctl) { ctl->loops++; }
+// condition of an IF node: the control state equals `when`
+__global__ void k_set_if(const KCtl* ctl, cudaGraphConditionalHandle h, int when) {
+    cudaGraphSetConditional(h, ctl->state == when ? 1u : 0u);
+}
 
 // ---------------------------------------------------------------------------
 // generic fused vector kernel:  y = sum_i c_i x_i  (+ y if acc), c_i from slots;
@@ -270,7 +384,8 @@ __device__ __forceinline__ double2 eval_coef(const CoefSpec& c, const double2* S
 
 template <typename C, int NT, int K>
 __global__ void __launch_bounds__(256) k_lin(LinArgs<C, NT, K> g, long long n, const double2* __restrict__ S,
-                                             double2* __restrict__ partial) {
+                                             double2* __restrict__ partial, Gate gate) {
+    if (gate_closed(gate)) return;
     C cf[NT];
 #pragma unroll
     for (int i = 0; i < NT; i++) cf[i] = coef_c<C>(eval_coef(g.t[i].c, S));
@@ -300,7 +415,9 @@ template <typename C, int K> struct DotArgs {
     int conj[K];
 };
 template <typename C, int K>
-__global__ void __launch_bounds__(256) k_dots(DotArgs<C, K> g, long long n, double2* __restrict__ partial) {
+__global__ void __launch_bounds__(256) k_dots(DotArgs<C, K> g, long long n, double2* __restrict__ partial,
+                                              Gate gate) {
+    if (gate_closed(gate)) return;
     double2 acc[K];
 #pragma unroll
     for (int k = 0; k < K; k++) acc[k] = make_double2(0, 0);
@@ -350,13 +467,15 @@ __global__ void k_scale_to(C* __restrict__ y, const double2* __restrict__ x, lon
 }
 
 // y32 = float(x64)
-__global__ void k_to_f32(float2* __restrict__ y, const double2* __restrict__ x, long long n) {
+__global__ void k_to_f32(float2* __restrict__ y, const double2* __restrict__ x, long long n, Gate gate) {
+    if (gate_closed(gate)) return;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
         y[i] = make_float2((float)x[i].x, (float)x[i].y);
 }
 
 // x64 += x32; x32 = 0 (the FP64 solution update of a reliable-update step)
-__global__ void k_fold_correction(double2* __restrict__ x64, float2* __restrict__ x32, long long n) {
+__global__ void k_fold_correction(double2* __restrict__ x64, float2* __restrict__ x32, long long n, Gate gate) {
+    if (gate_closed(gate)) return;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         const float2 d = x32[i];
         double2 v = x64[i];
@@ -469,7 +588,9 @@ template <typename C>
 __global__ void __launch_bounds__(256) k_bicgstab_update(C* __restrict__ x, const C* __restrict__ p,
                                                          const C* __restrict__ sv, const C* __restrict__ t,
                                                          C* __restrict__ r, const C* __restrict__ b, long long n,
-                                                         const double2* __restrict__ S, double2* __restrict__ partial) {
+                                                         const double2* __restrict__ S, double2* __restrict__ partial,
+                                                         Gate gate) {
+    if (gate_closed(gate)) return;
     const C alpha = from_d2<C>(S[S_ALPHA]), omega = from_d2<C>(S[S_OMEGA]);
     double2 acc[2] = {make_double2(0, 0), make_double2(0, 0)};
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
@@ -524,7 +645,7 @@ static void* work_vec(vie_ctx* ctx, int idx, size_t elem, int* rc) {
 
 template <int K, class Fin>
 static int finalize(vie_ctx* ctx, long long nblk, Fin fin) {
-    k_finalize<K, Fin><<<1, 256, 0, ctx->stream>>>(ctx->d_partial, nblk, ctx->d_scal, fin);
+    k_finalize<K, Fin><<<1, 256, 0, ctx->stream>>>(ctx->d_partial, nblk, ctx->d_scal, fin, ctx->gate);
     count_launch();
     VIE_CUDA_TRY(cudaGetLastError(), ctx->err);
     return VIE_OK;
@@ -532,7 +653,7 @@ static int finalize(vie_ctx* ctx, long long nblk, Fin fin) {
 
 template <typename C, int NT, int K>
 static int lin(vie_ctx* ctx, const LinArgs<C, NT, K>& g) {
-    k_lin<C, NT, K><<<kVecBlocks, 256, 0, ctx->stream>>>(g, 3 * ctx->a, ctx->d_scal, ctx->d_partial);
+    k_lin<C, NT, K><<<kVecBlocks, 256, 0, ctx->stream>>>(g, 3 * ctx->a, ctx->d_scal, ctx->d_partial, ctx->gate);
     count_launch();
     VIE_CUDA_TRY(cudaGetLastError(), ctx->err);
     return VIE_OK;
@@ -540,7 +661,7 @@ static int lin(vie_ctx* ctx, const LinArgs<C, NT, K>& g) {
 
 template <typename C, int K>
 static int dots(vie_ctx* ctx, const DotArgs<C, K>& g) {
-    k_dots<C, K><<<kVecBlocks, 256, 0, ctx->stream>>>(g, 3 * ctx->a, ctx->d_partial);
+    k_dots<C, K><<<kVecBlocks, 256, 0, ctx->stream>>>(g, 3 * ctx->a, ctx->d_partial, ctx->gate);
     count_launch();
     VIE_CUDA_TRY(cudaGetLastError(), ctx->err);
     return VIE_OK;
@@ -565,15 +686,263 @@ struct KrylovResult {
     int status = VIE_OK;
 };
 
-// matvec with generic prologue/epilogue on operator op
+// matvec with generic prologue/epilogue on operator op, under the current gate
 template <typename T, class Pro, class Epi>
 static int opmv(vie_ctx* ctx, Operator<T>& op, Pro pro, Epi epi, const cplx_t<T>* xdiag, bool conj) {
-    return launch_operator<T>(op, pro, epi, xdiag, conj, ctx->d_partial, ctx->stream, ctx->err);
+    op.dev.gate = ctx->gate;
+    const int rc = launch_operator<T>(op, pro, epi, xdiag, conj, ctx->d_partial, ctx->stream, ctx->err);
+    op.dev.gate = Gate{nullptr, 0};
+    return rc;
+}
+
+// ---------------------------------------------------------------------------
+// control block and the iteration loop
+// ---------------------------------------------------------------------------
+__global__ void k_ctl_init(KCtl* c, double thr, int maxit, double delta, int cap) {
+    KCtl v;
+    v.state = KS_RUN;
+    v.iter = 0;
+    v.maxit = maxit;
+    v.steps = -1;
+    v.updates = 0;
+    v.loops = 0;
+    v.hist_cap = cap;
+    v.pad = 0;
+    v.thr = thr;
+    v.delta = delta;
+    v.rmax2 = 0.0;
+    v.bn2 = 0.0;
+    v.last = -1.0;
+    *c = v;
+}
+
+// state RUN, counters zero; the history holds up to 2^20 iterations
+static int ctl_init(vie_ctx* ctx, double thr, int maxit, double delta) {
+    if (!ctx->d_ctl) {
+        VIE_CUDA_TRY(cudaMalloc(&ctx->d_ctl, sizeof(KCtl)), ctx->err);
+        VIE_CUDA_TRY(cudaMallocHost(&ctx->h_ctl, sizeof(KCtl)), ctx->err);
+    }
+    const int cap = (int)std::min<long long>(std::max(maxit, 1), 1LL << 20);
+    if (ctx->hist_cap < cap) {
+        if (ctx->d_hist) cudaFree(ctx->d_hist);
+        ctx->d_hist = nullptr;
+        ctx->hist_cap = 0;
+        VIE_CUDA_TRY(cudaMalloc(&ctx->d_hist, sizeof(double2) * cap), ctx->err);
+        ctx->hist_cap = cap;
+    }
+    k_ctl_init<<<1, 1, 0, ctx->stream>>>(ctx->d_ctl, thr, maxit, delta, ctx->hist_cap);
+    count_launch();
+    VIE_CUDA_TRY(cudaGetLastError(), ctx->err);
+    return VIE_OK;
+}
+
+static int ctl_read(vie_ctx* ctx) {
+    VIE_CUDA_TRY(cudaMemcpyAsync(ctx->h_ctl, ctx->d_ctl, sizeof(KCtl), cudaMemcpyDeviceToHost, ctx->stream), ctx->err);
+    VIE_CUDA_TRY(cudaStreamSynchronize(ctx->stream), ctx->err);
+    return VIE_OK;
+}
+
+static bool ks_live(int s) { return s == KS_RUN || s == KS_UPDATE || s == KS_RESET; }
+
+// Launches enqueued between cond_begin(when) and cond_end run only while the
+// control state equals `when`.  Inside a captured body they become the child
+// graph of a conditional IF node, so they are not launched at all otherwise;
+// outside a capture their gates alone skip them.
+static int cond_begin(vie_ctx* ctx, int when) {
+    if (!ctx->capturing) return VIE_OK;
+    cudaStream_t st = ctx->stream;
+    cudaStreamCaptureStatus cst;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    VIE_CUDA_TRY(cudaStreamGetCaptureInfo(st, &cst, nullptr, &g, &deps, &nd), ctx->err);
+    cudaGraphConditionalHandle h;
+    VIE_CUDA_TRY(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault), ctx->err);
+    k_set_if<<<1, 1, 0, st>>>(ctx->d_ctl, h, when);
+    count_launch();
+    VIE_CUDA_TRY(cudaGetLastError(), ctx->err);
+    VIE_CUDA_TRY(cudaStreamGetCaptureInfo(st, &cst, nullptr, &g, &deps, &nd), ctx->err);
+    cudaGraphNodeParams np = {cudaGraphNodeTypeConditional};
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeIf;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    VIE_CUDA_TRY(cudaGraphAddNode(&node, g, deps, nd, &np), ctx->err);
+    VIE_CUDA_TRY(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies), ctx->err);
+    if (!ctx->stream_aux)
+        VIE_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->stream_aux, cudaStreamNonBlocking), ctx->err);
+    VIE_CUDA_TRY(cudaStreamBeginCaptureToGraph(ctx->stream_aux, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                               cudaStreamCaptureModeRelaxed),
+                 ctx->err);
+    ctx->stream_parent = st;
+    ctx->stream = ctx->stream_aux;
+    return VIE_OK;
+}
+static int cond_end(vie_ctx* ctx) {
+    if (!ctx->capturing || !ctx->stream_parent) return VIE_OK;
+    cudaGraph_t g = nullptr;
+    ctx->stream = ctx->stream_parent;
+    ctx->stream_parent = nullptr;
+    VIE_CUDA_TRY(cudaStreamEndCapture(ctx->stream_aux, &g), ctx->err);
+    return VIE_OK;
+}
+
+// Graph form of the loop: the body is captured once as the child graph of a
+// conditional WHILE node whose condition k_loop_cond sets from the control
+// state after every pass, so the whole solve is one graph launch.  Returns
+// an error with launched == false when the graph could not be built (nothing
+// of the body ran then).
+template <class Body>
+static int run_loop_graph(vie_ctx* ctx, Body& body, bool& launched) {
+    cudaStream_t st = ctx->stream;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int rc = VIE_OK;
+    launched = false;
+    do {
+        cudaGraphConditionalHandle h;
+        if (cudaGraphCreate(&graph, 0) != cudaSuccess ||
+            cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault) != cudaSuccess) {
+            rc = ctx->set_error(VIE_ERR_CUDA, "conditional graph handle");
+            break;
+        }
+        cudaGraphNodeParams np = {cudaGraphNodeTypeConditional};
+        np.conditional.handle = h;
+        np.conditional.type = cudaGraphCondTypeWhile;
+        np.conditional.size = 1;
+        cudaGraphNode_t node;
+        if (cudaGraphAddNode(&node, graph, nullptr, 0, &np) != cudaSuccess) {
+            rc = ctx->set_error(VIE_ERR_CUDA, "conditional WHILE node");
+            break;
+        }
+        cudaGraph_t bodyg = np.conditional.phGraph_out[0];
+        if (cudaStreamBeginCaptureToGraph(st, bodyg, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) != cudaSuccess) {
+            rc = ctx->set_error(VIE_ERR_CUDA, "stream capture into the loop body");
+            break;
+        }
+        const long long n0 = g_launches.load();
+        ctx->capturing = 1;
+        int brc = body();
+        if (ctx->stream_parent) {  // an IF body left open by an error
+            cudaGraph_t tmp = nullptr;
+            cudaStreamEndCapture(ctx->stream_aux, &tmp);
+            ctx->stream = ctx->stream_parent;
+            ctx->stream_parent = nullptr;
+        }
+        ctx->capturing = 0;
+        k_loop_cond<<<1, 1, 0, st>>>(ctx->d_ctl, h);
+        count_launch();
+        cudaGraph_t captured = nullptr;
+        const cudaError_t ce = cudaStreamEndCapture(st, &captured);
+        const long long per = g_launches.load() - n0;
+        count_launch(-per);  // counted again below, once per executed pass
+        if (brc) { rc = brc; break; }
+        if (ce != cudaSuccess) {
+            rc = ctx->set_error(VIE_ERR_CUDA, std::string("stream capture of the loop body: ") + cudaGetErrorString(ce));
+            break;
+        }
+        if (cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) {
+            rc = ctx->set_error(VIE_ERR_CUDA, "graph instantiation");
+            break;
+        }
+        launched = true;
+        VIE_CUDA_TRY(cudaGraphLaunch(exec, st), ctx->err);
+        if ((rc = ctl_read(ctx))) break;
+        count_launch(per * ctx->h_ctl->loops);
+        ctx->graph_launches++;
+    } while (0);
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (rc && !launched) (void)cudaGetLastError();  // clear a non-sticky build error
+    return rc;
+}
+
+// Runs the iteration body until the control state is terminal: as one graph
+// launch (default), or, with VIE_GRAPH=0 or where the graph cannot be built,
+// launched from the host with the state read back after every pass.
+template <class Body>
+static int run_loop(vie_ctx* ctx, Body body) {
+    if (ctx->use_graphs) {
+        bool launched = false;
+        const int rc = run_loop_graph(ctx, body, launched);
+        if (launched || rc == VIE_OK) return rc;
+        // the graph could not be built (nothing ran): the same body from the host
+        std::fprintf(stderr, "vie_b200: %s; iterating without graphs\n", ctx->err.msg.c_str());
+        ctx->err.code = VIE_OK;
+        ctx->use_graphs = 0;
+    }
+    cudaStream_t st = ctx->stream;
+    while (true) {
+        int rc = body();
+        if (rc) return rc;
+        k_loop_count<<<1, 1, 0, st>>>(ctx->d_ctl);
+        count_launch();
+        VIE_CUDA_TRY(cudaGetLastError(), ctx->err);
+        if ((rc = ctl_read(ctx))) return rc;
+        if (!ks_live(ctx->h_ctl->state)) return VIE_OK;
+    }
+}
+
+// the drivers' console output, replayed from the device history:
+// "CG Error" per step, "Steps" at convergence (CG_Iteration.h:323-331 etc.);
+// BiCORSTAB prints only "Steps" at convergence (:1315-1327); the mixed solve
+// prints the true residual of every reliable update
+enum PrintStyle { PS_ERR_STEPS = 0, PS_STEPS_ONLY = 1, PS_RELIABLE = 2 };
+static int print_history(vie_ctx* ctx, const KCtl& c, int style) {
+    const int n = std::min(c.iter, c.hist_cap);
+    if (n <= 0) return VIE_OK;
+    std::vector<double2> h((size_t)n);
+    VIE_CUDA_TRY(cudaMemcpy(h.data(), ctx->d_hist, sizeof(double2) * n, cudaMemcpyDeviceToHost), ctx->err);
+    for (int m = 0; m < n; m++) {
+        if (style == PS_RELIABLE) {
+            if (h[m].y >= 0.0) printf("CG Error: %lf (true residual)\n", h[m].y);
+            else printf("CG Error: %lf\n", h[m].x);
+        } else if (c.state == KS_DONE && m == c.steps) {
+            if (style == PS_ERR_STEPS) printf("CG Error: %lf\nSteps: %d\n\n", h[m].x, m);
+            else printf("Steps: %d\n\n", m);
+        } else {
+            printf("CG Error: %lf\n", h[m].x);
+        }
+    }
+    fflush(stdout);
+    return VIE_OK;
+}
+
+// outcome of a loop from the control block (already read back)
+static int finish(vie_ctx* ctx, KrylovResult& res, int mv_setup, int mv_per_iter, int style, int verbose,
+                  const char* name) {
+    const KCtl c = *ctx->h_ctl;
+    if (verbose) {
+        const int rc = print_history(ctx, c, style);
+        if (rc) return rc;
+    }
+    res.iterations = c.iter;
+    res.matvecs = mv_setup + mv_per_iter * c.iter;
+    res.err = c.last;
+    if (c.state == KS_DONE) {
+        res.steps = c.steps;
+        return VIE_OK;
+    }
+    if (c.state == KS_MAXIT) {
+        res.status = VIE_ERR_MAXIT;
+        return VIE_OK;
+    }
+    res.status = VIE_ERR_BREAKDOWN;
+    return ctx->set_error(VIE_ERR_BREAKDOWN, std::string(name) + " breakdown (zero or non-finite scalar) at step " +
+                                                 std::to_string(c.iter - 1));
+}
+
+static int zero_vecs(vie_ctx* ctx, size_t bytes, std::initializer_list<void*> vs) {
+    for (void* v : vs) VIE_CUDA_TRY(cudaMemsetAsync(v, 0, bytes, ctx->stream), ctx->err);
+    return VIE_OK;
 }
 
 // ---------------------------------------------------------------------------
 // solvers on C-precision vectors.  b: masked right-hand side, x: solution
-// (zeroed here), thr: threshold on the solver's own error measure.
+// (zeroed here), thr: threshold on the solver's own error measure.  Each one
+// is a set-up followed by an iteration body whose first pass equals the
+// reference's first step because the direction vectors start at zero and
+// beta at 0.
 // ---------------------------------------------------------------------------
 template <typename T>
 static int solve_bicgstab(vie_ctx* ctx, Operator<T>& op, const cplx_t<T>* b, cplx_t<T>* x, double thr, int maxit,
@@ -588,47 +957,35 @@ static int solve_bicgstab(vie_ctx* ctx, Operator<T>& op, const cplx_t<T>* b, cpl
     C* t = (C*)work_vec(ctx, vbase + 4, sizeof(C), &rc);
     if (rc) return rc;
     cudaStream_t st = ctx->stream;
-    VIE_CUDA_TRY(cudaMemsetAsync(x, 0, sizeof(C) * n, st), ctx->err);
+    if ((rc = zero_vecs(ctx, sizeof(C) * n, {x, p, v}))) return rc;
     VIE_CUDA_TRY(cudaMemcpyAsync(r, b, sizeof(C) * n, cudaMemcpyDeviceToDevice, st), ctx->err);  // :565-567
     {
         DotArgs<C, 2> g{{b, b}, {b, r}, {1, 1}};
         if ((rc = dots(ctx, g))) return rc;
         if ((rc = finalize<2>(ctx, kVecBlocks, FinBicgstabInit{}))) return rc;
     }
+    if ((rc = ctl_init(ctx, thr, maxit, 0.0))) return rc;
+    KCtl* ctl = ctx->d_ctl;
+    double2* hist = ctx->d_hist;
     const long long nblk = epilogue_blocks(op);
-    for (int m = 0; m < maxit; m++) {
-        if (m == 0) {
-            if ((rc = opmv(ctx, op, ProCopyWrite<C>{r, p, a}, EpiDotB<C>{v, b, a}, p, false))) return rc;
-        } else {
-            if ((rc = opmv(ctx, op, ProBicgP<C>{r, p, v, ctx->d_scal, a}, EpiDotB<C>{v, b, a}, p, false))) return rc;
-        }
-        if ((rc = finalize<1>(ctx, nblk, FinAlpha{}))) return rc;
-        if ((rc = opmv(ctx, op, ProBicgS<C>{r, v, sv, ctx->d_scal, a}, EpiDotTS<C>{t, sv, a}, sv, false))) return rc;
-        if ((rc = finalize<2>(ctx, nblk, FinOmega{}))) return rc;
-        k_bicgstab_update<C><<<kVecBlocks, 256, 0, st>>>(x, p, sv, t, r, b, n, ctx->d_scal, ctx->d_partial);
+    auto body = [&]() -> int {
+        int rc2;
+        ctx->gate = Gate{&ctl->state, KS_RUN};
+        // p = r + beta (p - omega v) (:611-633); v = A p; b^H v (:652-662)
+        if ((rc2 = opmv(ctx, op, ProBicgP<C>{r, p, v, ctx->d_scal, a}, EpiDotB<C>{v, b, a}, p, false))) return rc2;
+        if ((rc2 = finalize<1>(ctx, nblk, FinAlpha{}))) return rc2;
+        // s = r - alpha v (:664-672); t = A s; t^H s, t^H t (:689-706)
+        if ((rc2 = opmv(ctx, op, ProBicgS<C>{r, v, sv, ctx->d_scal, a}, EpiDotTS<C>{t, sv, a}, sv, false))) return rc2;
+        if ((rc2 = finalize<2>(ctx, nblk, FinOmega{}))) return rc2;
+        k_bicgstab_update<C><<<kVecBlocks, 256, 0, st>>>(x, p, sv, t, r, b, n, ctx->d_scal, ctx->d_partial, ctx->gate);
         count_launch();
         VIE_CUDA_TRY(cudaGetLastError(), ctx->err);
-        if ((rc = finalize<2>(ctx, kVecBlocks, FinBicgstabUpdate{}))) return rc;
-        res.matvecs += 2;
-        res.iterations = m + 1;
-        if ((rc = read_scalars(ctx))) return rc;
-        const double err = ctx->h_scal[S_ERR].x;
-        res.err = err;
-        if (ctx->h_scal[S_NAN].x != 0.0) {
-            if (err < thr) { res.steps = m; return VIE_OK; }
-            res.status = VIE_ERR_BREAKDOWN;
-            return ctx->set_error(VIE_ERR_BREAKDOWN, "BiCGSTAB breakdown (zero or non-finite scalar) at step " +
-                                                         std::to_string(m));
-        }
-        if (err < thr) {
-            if (verbose) printf("CG Error: %lf\nSteps: %d\n\n", err, m);
-            res.steps = m;
-            return VIE_OK;
-        }
-        if (verbose) printf("CG Error: %lf\n", err);
-    }
-    res.status = VIE_ERR_MAXIT;
-    return VIE_OK;
+        return finalize<2>(ctx, kVecBlocks, then(FinBicgstabUpdate{}, DecideErr{ctl, hist}));
+    };
+    rc = run_loop(ctx, body);
+    ctx->gate = Gate{nullptr, 0};
+    if (rc) return rc;
+    return finish(ctx, res, 0, 2, PS_ERR_STEPS, verbose, "BiCGSTAB");
 }
 
 template <typename T>
@@ -647,57 +1004,44 @@ static int solve_cors(vie_ctx* ctx, Operator<T>& op, const cplx_t<T>* b, cplx_t<
     C* qc = (C*)work_vec(ctx, vbase + 7, sizeof(C), &rc);
     if (rc) return rc;
     cudaStream_t st = ctx->stream;
-    VIE_CUDA_TRY(cudaMemsetAsync(x, 0, sizeof(C) * n, st), ctx->err);
+    if ((rc = zero_vecs(ctx, sizeof(C) * n, {x, q, rc_, pc}))) return rc;
     VIE_CUDA_TRY(cudaMemcpyAsync(r, b, sizeof(C) * n, cudaMemcpyDeviceToDevice, st), ctx->err);  // :826-828
     {
         DotArgs<C, 1> g{{b}, {b}, {1}};
         if ((rc = dots(ctx, g))) return rc;
         if ((rc = finalize<1>(ctx, kVecBlocks, FinStore1{S_BNRM2}))) return rc;
     }
+    if ((rc = ctl_init(ctx, thr, maxit, 0.0))) return rc;
+    KCtl* ctl = ctx->d_ctl;
+    double2* hist = ctx->d_hist;
     const long long nblk = epilogue_blocks(op);
-    for (int m = 0; m < maxit; m++) {
+    auto body = [&]() -> int {
+        int rc2;
+        ctx->gate = Gate{&ctl->state, KS_RUN};
         // Ap = A r; rho = b^H Ap (:853-869)
-        if ((rc = opmv(ctx, op, ProCopy<C>{r, a}, EpiDotB<C>{Ap, b, a}, r, false))) return rc;
-        if ((rc = finalize<1>(ctx, nblk, FinCorsRho{m == 0}))) return rc;
-        if (m > 0) {
-            // p = r + beta pc; qc = Ap + beta rc; q = qc + beta rc + beta^2 q  (:880-915)
-            if ((rc = lin(ctx, LinArgs<C, 2, 0>{p, 0, {{r, cs(-1)}, {pc, cs(S_BETA)}}, {}}))) return rc;
-            if ((rc = lin(ctx, LinArgs<C, 2, 0>{qc, 0, {{Ap, cs(-1)}, {rc_, cs(S_BETA)}}, {}}))) return rc;
-            if ((rc = lin(ctx, LinArgs<C, 3, 0>{q, 0, {{q, cs(S_T0)}, {rc_, cs(S_BETA)}, {qc, cs(-1)}}, {}}))) return rc;
-        } else {
-            VIE_CUDA_TRY(cudaMemcpyAsync(p, r, sizeof(C) * n, cudaMemcpyDeviceToDevice, st), ctx->err);
-            VIE_CUDA_TRY(cudaMemcpyAsync(qc, Ap, sizeof(C) * n, cudaMemcpyDeviceToDevice, st), ctx->err);
-            VIE_CUDA_TRY(cudaMemcpyAsync(q, Ap, sizeof(C) * n, cudaMemcpyDeviceToDevice, st), ctx->err);
-        }
+        if ((rc2 = opmv(ctx, op, ProCopy<C>{r, a}, EpiDotB<C>{Ap, b, a}, r, false))) return rc2;
+        if ((rc2 = finalize<1>(ctx, nblk, FinCorsRho{ctl}))) return rc2;
+        // p = r + beta pc; qc = Ap + beta rc; q = qc + beta rc + beta^2 q (:880-915);
+        // on the first step beta = 0 and pc = rc = q = 0: p = r, qc = q = Ap (:843-851)
+        if ((rc2 = lin(ctx, LinArgs<C, 2, 0>{p, 0, {{r, cs(-1)}, {pc, cs(S_BETA)}}, {}}))) return rc2;
+        if ((rc2 = lin(ctx, LinArgs<C, 2, 0>{qc, 0, {{Ap, cs(-1)}, {rc_, cs(S_BETA)}}, {}}))) return rc2;
+        if ((rc2 = lin(ctx, LinArgs<C, 3, 0>{q, 0, {{q, cs(S_T0)}, {rc_, cs(S_BETA)}, {qc, cs(-1)}}, {}}))) return rc2;
         // Aq = A q; alpha = rho / (b^H Aq) (:938-962)
-        if ((rc = opmv(ctx, op, ProCopy<C>{q, a}, EpiDotB<C>{Aq, b, a}, q, false))) return rc;
-        if ((rc = finalize<1>(ctx, nblk, FinCorsAlpha{}))) return rc;
+        if ((rc2 = opmv(ctx, op, ProCopy<C>{q, a}, EpiDotB<C>{Aq, b, a}, q, false))) return rc2;
+        if ((rc2 = finalize<1>(ctx, nblk, FinCorsAlpha{}))) return rc2;
         // pc = p - alpha q; rc = qc - alpha Aq (:964-981)
-        if ((rc = lin(ctx, LinArgs<C, 2, 0>{pc, 0, {{p, cs(-1)}, {q, cs(S_ALPHA, -1.0)}}, {}}))) return rc;
-        if ((rc = lin(ctx, LinArgs<C, 2, 0>{rc_, 0, {{qc, cs(-1)}, {Aq, cs(S_ALPHA, -1.0)}}, {}}))) return rc;
+        if ((rc2 = lin(ctx, LinArgs<C, 2, 0>{pc, 0, {{p, cs(-1)}, {q, cs(S_ALPHA, -1.0)}}, {}}))) return rc2;
+        if ((rc2 = lin(ctx, LinArgs<C, 2, 0>{rc_, 0, {{qc, cs(-1)}, {Aq, cs(S_ALPHA, -1.0)}}, {}}))) return rc2;
         // x += 2 alpha p - alpha^2 q (:983-997); r += -2 alpha qc + alpha^2 Aq (:999-1012); r^H r
-        if ((rc = lin(ctx, LinArgs<C, 2, 0>{x, 1, {{p, cs(S_ALPHA, 2.0)}, {q, cs(S_T1, -1.0)}}, {}}))) return rc;
-        if ((rc = lin(ctx, LinArgs<C, 2, 1>{r, 1, {{qc, cs(S_ALPHA, -2.0)}, {Aq, cs(S_T1)}}, {{nullptr, 1}}})))
-            return rc;
-        if ((rc = finalize<1>(ctx, kVecBlocks, FinErr{}))) return rc;
-        res.matvecs += 2;
-        res.iterations = m + 1;
-        if ((rc = read_scalars(ctx))) return rc;
-        const double err = ctx->h_scal[S_ERR].x;
-        res.err = err;
-        if (ctx->h_scal[S_NAN].x != 0.0 && !(err < thr)) {
-            res.status = VIE_ERR_BREAKDOWN;
-            return ctx->set_error(VIE_ERR_BREAKDOWN, "CORS breakdown at step " + std::to_string(m));
-        }
-        if (err < thr) {
-            if (verbose) printf("CG Error: %lf\nSteps: %d\n\n", err, m);
-            res.steps = m;
-            return VIE_OK;
-        }
-        if (verbose) printf("CG Error: %lf\n", err);
-    }
-    res.status = VIE_ERR_MAXIT;
-    return VIE_OK;
+        if ((rc2 = lin(ctx, LinArgs<C, 2, 0>{x, 1, {{p, cs(S_ALPHA, 2.0)}, {q, cs(S_T1, -1.0)}}, {}}))) return rc2;
+        if ((rc2 = lin(ctx, LinArgs<C, 2, 1>{r, 1, {{qc, cs(S_ALPHA, -2.0)}, {Aq, cs(S_T1)}}, {{nullptr, 1}}})))
+            return rc2;
+        return finalize<1>(ctx, kVecBlocks, then(FinErr{}, DecideErr{ctl, hist}));
+    };
+    rc = run_loop(ctx, body);
+    ctx->gate = Gate{nullptr, 0};
+    if (rc) return rc;
+    return finish(ctx, res, 0, 2, PS_ERR_STEPS, verbose, "CORS");
 }
 
 template <typename T>
@@ -715,57 +1059,46 @@ static int solve_bicorstab(vie_ctx* ctx, Operator<T>& op, const cplx_t<T>* b, cp
     C* qc = (C*)work_vec(ctx, vbase + 6, sizeof(C), &rc);
     if (rc) return rc;
     cudaStream_t st = ctx->stream;
-    VIE_CUDA_TRY(cudaMemsetAsync(x, 0, sizeof(C) * n, st), ctx->err);
+    if ((rc = zero_vecs(ctx, sizeof(C) * n, {x, p, q, Aq}))) return rc;
     VIE_CUDA_TRY(cudaMemcpyAsync(r, b, sizeof(C) * n, cudaMemcpyDeviceToDevice, st), ctx->err);  // :1118-1120
     {
         DotArgs<C, 1> g{{b}, {b}, {1}};
         if ((rc = dots(ctx, g))) return rc;
         if ((rc = finalize<1>(ctx, kVecBlocks, FinStore1{S_BNRM2}))) return rc;
     }
+    if ((rc = ctl_init(ctx, thr, maxit, 0.0))) return rc;
+    KCtl* ctl = ctx->d_ctl;
+    double2* hist = ctx->d_hist;
     const long long nblk = epilogue_blocks(op);
-    for (int m = 0; m < maxit; m++) {
-        if ((rc = opmv(ctx, op, ProCopy<C>{r, a}, EpiDotB<C>{Ap, b, a}, r, false))) return rc;   // :1145-1162
-        if ((rc = finalize<1>(ctx, nblk, FinBicorRho{m == 0}))) return rc;
-        if (m > 0) {
-            // p = r + beta (p - omega q); q = Ap + beta (q - omega Aq)  (:1175-1207)
-            if ((rc = lin(ctx, LinArgs<C, 3, 0>{p, 0, {{p, cs(S_BETA)}, {q, cs(S_T2, -1.0)}, {r, cs(-1)}}, {}})))
-                return rc;
-            if ((rc = lin(ctx, LinArgs<C, 3, 0>{q, 0, {{q, cs(S_BETA)}, {Aq, cs(S_T2, -1.0)}, {Ap, cs(-1)}}, {}})))
-                return rc;
-        } else {
-            VIE_CUDA_TRY(cudaMemcpyAsync(p, r, sizeof(C) * n, cudaMemcpyDeviceToDevice, st), ctx->err);
-            VIE_CUDA_TRY(cudaMemcpyAsync(q, Ap, sizeof(C) * n, cudaMemcpyDeviceToDevice, st), ctx->err);
-        }
-        if ((rc = opmv(ctx, op, ProCopy<C>{q, a}, EpiDotB<C>{Aq, b, a}, q, false))) return rc;   // :1224-1248
-        if ((rc = finalize<1>(ctx, nblk, FinAlpha{}))) return rc;
+    auto body = [&]() -> int {
+        int rc2;
+        ctx->gate = Gate{&ctl->state, KS_RUN};
+        if ((rc2 = opmv(ctx, op, ProCopy<C>{r, a}, EpiDotB<C>{Ap, b, a}, r, false))) return rc2;   // :1145-1162
+        if ((rc2 = finalize<1>(ctx, nblk, FinBicorRho{ctl}))) return rc2;
+        // p = r + beta (p - omega q); q = Ap + beta (q - omega Aq)  (:1175-1207);
+        // first step: beta = 0 and p = q = Aq = 0 give p = r, q = Ap (:1134-1143)
+        if ((rc2 = lin(ctx, LinArgs<C, 3, 0>{p, 0, {{p, cs(S_BETA)}, {q, cs(S_T2, -1.0)}, {r, cs(-1)}}, {}})))
+            return rc2;
+        if ((rc2 = lin(ctx, LinArgs<C, 3, 0>{q, 0, {{q, cs(S_BETA)}, {Aq, cs(S_T2, -1.0)}, {Ap, cs(-1)}}, {}})))
+            return rc2;
+        if ((rc2 = opmv(ctx, op, ProCopy<C>{q, a}, EpiDotB<C>{Aq, b, a}, q, false))) return rc2;   // :1224-1248
+        if ((rc2 = finalize<1>(ctx, nblk, FinAlpha{}))) return rc2;
         // pc = r - alpha q; qc = Ap - alpha Aq; omega = qc^H pc / qc^H qc  (:1250-1287)
-        if ((rc = lin(ctx, LinArgs<C, 2, 0>{pc, 0, {{r, cs(-1)}, {q, cs(S_ALPHA, -1.0)}}, {}}))) return rc;
-        if ((rc = lin(ctx, LinArgs<C, 2, 2>{qc, 0, {{Ap, cs(-1)}, {Aq, cs(S_ALPHA, -1.0)}}, {{pc, 1}, {nullptr, 1}}})))
-            return rc;
+        if ((rc2 = lin(ctx, LinArgs<C, 2, 0>{pc, 0, {{r, cs(-1)}, {q, cs(S_ALPHA, -1.0)}}, {}}))) return rc2;
+        if ((rc2 = lin(ctx, LinArgs<C, 2, 2>{qc, 0, {{Ap, cs(-1)}, {Aq, cs(S_ALPHA, -1.0)}}, {{pc, 1}, {nullptr, 1}}})))
+            return rc2;
         // d0 = conj(pc).qc, so qc^H pc = conj(d0)
-        if ((rc = finalize<2>(ctx, kVecBlocks, FinBicorOmega{}))) return rc;
+        if ((rc2 = finalize<2>(ctx, kVecBlocks, FinBicorOmega{}))) return rc2;
         // x += alpha p + omega pc; r = pc - omega qc; r^H r  (:1289-1315)
-        if ((rc = lin(ctx, LinArgs<C, 2, 0>{x, 1, {{p, cs(S_ALPHA)}, {pc, cs(S_OMEGA)}}, {}}))) return rc;
-        if ((rc = lin(ctx, LinArgs<C, 2, 1>{r, 0, {{pc, cs(-1)}, {qc, cs(S_OMEGA, -1.0)}}, {{nullptr, 1}}}))) return rc;
-        if ((rc = finalize<1>(ctx, kVecBlocks, FinErr{}))) return rc;
-        res.matvecs += 2;
-        res.iterations = m + 1;
-        if ((rc = read_scalars(ctx))) return rc;
-        const double err = ctx->h_scal[S_ERR].x;
-        res.err = err;
-        if (ctx->h_scal[S_NAN].x != 0.0 && !(err < thr)) {
-            res.status = VIE_ERR_BREAKDOWN;
-            return ctx->set_error(VIE_ERR_BREAKDOWN, "BiCORSTAB breakdown at step " + std::to_string(m));
-        }
-        if (err < thr) {
-            if (verbose) printf("Steps: %d\n\n", m);
-            res.steps = m;
-            return VIE_OK;
-        }
-        if (verbose) printf("CG Error: %lf\n", err);
-    }
-    res.status = VIE_ERR_MAXIT;
-    return VIE_OK;
+        if ((rc2 = lin(ctx, LinArgs<C, 2, 0>{x, 1, {{p, cs(S_ALPHA)}, {pc, cs(S_OMEGA)}}, {}}))) return rc2;
+        if ((rc2 = lin(ctx, LinArgs<C, 2, 1>{r, 0, {{pc, cs(-1)}, {qc, cs(S_OMEGA, -1.0)}}, {{nullptr, 1}}})))
+            return rc2;
+        return finalize<1>(ctx, kVecBlocks, then(FinErr{}, DecideErr{ctl, hist}));
+    };
+    rc = run_loop(ctx, body);
+    ctx->gate = Gate{nullptr, 0};
+    if (rc) return rc;
+    return finish(ctx, res, 0, 2, PS_STEPS_ONLY, verbose, "BiCORSTAB");
 }
 
 template <typename T>
@@ -779,8 +1112,7 @@ static int solve_cg(vie_ctx* ctx, Operator<T>& op, const cplx_t<T>* b, cplx_t<T>
     C* q = (C*)work_vec(ctx, vbase + 2, sizeof(C), &rc);
     C* Ap = (C*)work_vec(ctx, vbase + 3, sizeof(C), &rc);
     if (rc) return rc;
-    cudaStream_t st = ctx->stream;
-    VIE_CUDA_TRY(cudaMemsetAsync(x, 0, sizeof(C) * n, st), ctx->err);
+    if ((rc = zero_vecs(ctx, sizeof(C) * n, {x}))) return rc;
     // r = -b (:208-216); p = A^H b (:219-229)
     if ((rc = lin(ctx, LinArgs<C, 1, 0>{r, 0, {{b, cs(-1, -1.0)}}, {}}))) return rc;
     if ((rc = opmv(ctx, op, ProCopy<C>{b, a}, EpiNorm<C>{p, a}, b, true))) return rc;
@@ -791,37 +1123,29 @@ static int solve_cg(vie_ctx* ctx, Operator<T>& op, const cplx_t<T>* b, cplx_t<T>
         if ((rc = dots(ctx, g))) return rc;
         if ((rc = finalize<1>(ctx, kVecBlocks, FinStore1{S_BNRM2}))) return rc;  // vx
     }
-    res.matvecs += 1;
-    for (int m = 0; m < maxit; m++) {
-        if ((rc = opmv(ctx, op, ProCopy<C>{p, a}, EpiNorm<C>{Ap, a}, p, false))) return rc;  // :253-268
-        if ((rc = finalize<1>(ctx, nblk, FinCgAlpha{}))) return rc;
+    if ((rc = ctl_init(ctx, thr, maxit, 0.0))) return rc;
+    KCtl* ctl = ctx->d_ctl;
+    double2* hist = ctx->d_hist;
+    auto body = [&]() -> int {
+        int rc2;
+        ctx->gate = Gate{&ctl->state, KS_RUN};
+        if ((rc2 = opmv(ctx, op, ProCopy<C>{p, a}, EpiNorm<C>{Ap, a}, p, false))) return rc2;  // :253-268
+        if ((rc2 = finalize<1>(ctx, nblk, FinCgAlpha{}))) return rc2;
         // x += alpha p; r += alpha Ap; v4 = ||r||^2 (:273-286)
-        if ((rc = lin(ctx, LinArgs<C, 1, 0>{x, 1, {{p, cs(S_ALPHA)}}, {}}))) return rc;
-        if ((rc = lin(ctx, LinArgs<C, 1, 1>{r, 1, {{Ap, cs(S_ALPHA)}}, {{nullptr, 1}}}))) return rc;
-        if ((rc = finalize<1>(ctx, kVecBlocks, FinCgErr{}))) return rc;
+        if ((rc2 = lin(ctx, LinArgs<C, 1, 0>{x, 1, {{p, cs(S_ALPHA)}}, {}}))) return rc2;
+        if ((rc2 = lin(ctx, LinArgs<C, 1, 1>{r, 1, {{Ap, cs(S_ALPHA)}}, {{nullptr, 1}}}))) return rc2;
+        if ((rc2 = finalize<1>(ctx, kVecBlocks, FinCgErr{}))) return rc2;
         // q = A^H r; v3 = ||q||^2; beta = v3 / v1 (:291-309)
-        if ((rc = opmv(ctx, op, ProCopy<C>{r, a}, EpiNorm<C>{q, a}, r, true))) return rc;
-        if ((rc = finalize<1>(ctx, nblk, FinCgBeta{}))) return rc;
-        // p = beta p - q (:311-320)
-        if ((rc = lin(ctx, LinArgs<C, 2, 0>{p, 0, {{p, cs(S_BETA)}, {q, cs(-1, -1.0)}}, {}}))) return rc;
-        res.matvecs += 2;
-        res.iterations = m + 1;
-        if ((rc = read_scalars(ctx))) return rc;
-        const double err = ctx->h_scal[S_ERR].x;
-        res.err = err;
-        if (ctx->h_scal[S_NAN].x != 0.0 && !(err < thr)) {
-            res.status = VIE_ERR_BREAKDOWN;
-            return ctx->set_error(VIE_ERR_BREAKDOWN, "CG breakdown at step " + std::to_string(m));
-        }
-        if (err < thr) {
-            if (verbose) printf("CG Error: %lf\nSteps: %d\n\n", err, m);
-            res.steps = m;
-            return VIE_OK;
-        }
-        if (verbose) printf("CG Error: %lf\n", err);
-    }
-    res.status = VIE_ERR_MAXIT;
-    return VIE_OK;
+        if ((rc2 = opmv(ctx, op, ProCopy<C>{r, a}, EpiNorm<C>{q, a}, r, true))) return rc2;
+        if ((rc2 = finalize<1>(ctx, nblk, FinCgBeta{}))) return rc2;
+        // p = beta p - q (:311-320); then the stop rule on v4 / vx (:323-331)
+        if ((rc2 = lin(ctx, LinArgs<C, 2, 0>{p, 0, {{p, cs(S_BETA)}, {q, cs(-1, -1.0)}}, {}}))) return rc2;
+        return finalize<1>(ctx, 1, then(FinNone{}, DecideErr{ctl, hist}));
+    };
+    rc = run_loop(ctx, body);
+    ctx->gate = Gate{nullptr, 0};
+    if (rc) return rc;
+    return finish(ctx, res, 1, 2, PS_ERR_STEPS, verbose, "CG");
 }
 
 template <typename T>
@@ -835,7 +1159,7 @@ static int solve_bicg(vie_ctx* ctx, Operator<T>& op, const cplx_t<T>* b, cplx_t<
     C* Ap = (C*)work_vec(ctx, vbase + 2, sizeof(C), &rc);
     if (rc) return rc;
     cudaStream_t st = ctx->stream;
-    VIE_CUDA_TRY(cudaMemsetAsync(x, 0, sizeof(C) * n, st), ctx->err);
+    if ((rc = zero_vecs(ctx, sizeof(C) * n, {x}))) return rc;
     VIE_CUDA_TRY(cudaMemcpyAsync(r, b, sizeof(C) * n, cudaMemcpyDeviceToDevice, st), ctx->err);  // :398-400
     {
         DotArgs<C, 1> g{{r}, {r}, {0}};
@@ -844,34 +1168,27 @@ static int solve_bicg(vie_ctx* ctx, Operator<T>& op, const cplx_t<T>* b, cplx_t<
     }
     // p = r / v1 (:413-424)
     if ((rc = lin(ctx, LinArgs<C, 1, 0>{p, 0, {{r, cs(S_T0)}}, {}}))) return rc;
+    if ((rc = ctl_init(ctx, thr, maxit, 0.0))) return rc;
+    KCtl* ctl = ctx->d_ctl;
+    double2* hist = ctx->d_hist;
     const long long nblk = epilogue_blocks(op);
-    for (int m = 0; m < maxit; m++) {
-        if ((rc = opmv(ctx, op, ProCopy<C>{p, a}, EpiDotU<C>{Ap, p, a}, p, false))) return rc;  // :437-453
-        if ((rc = finalize<1>(ctx, nblk, FinBicgAlpha{}))) return rc;
+    auto body = [&]() -> int {
+        int rc2;
+        ctx->gate = Gate{&ctl->state, KS_RUN};
+        if ((rc2 = opmv(ctx, op, ProCopy<C>{p, a}, EpiDotU<C>{Ap, p, a}, p, false))) return rc2;  // :437-453
+        if ((rc2 = finalize<1>(ctx, nblk, FinBicgAlpha{}))) return rc2;
         // x += alpha p; r -= alpha Ap; v2 = r^T r (:463-479)
-        if ((rc = lin(ctx, LinArgs<C, 1, 0>{x, 1, {{p, cs(S_ALPHA)}}, {}}))) return rc;
-        if ((rc = lin(ctx, LinArgs<C, 1, 1>{r, 1, {{Ap, cs(S_ALPHA, -1.0)}}, {{nullptr, 0}}}))) return rc;
-        if ((rc = finalize<1>(ctx, kVecBlocks, FinBicgBeta{}))) return rc;
-        // p += beta r (:489-491)
-        if ((rc = lin(ctx, LinArgs<C, 1, 0>{p, 1, {{r, cs(S_BETA)}}, {}}))) return rc;
-        res.matvecs += 1;
-        res.iterations = m + 1;
-        if ((rc = read_scalars(ctx))) return rc;
-        const double err = ctx->h_scal[S_ERR].x;
-        res.err = err;
-        if (ctx->h_scal[S_NAN].x != 0.0 && !(err < thr)) {
-            res.status = VIE_ERR_BREAKDOWN;
-            return ctx->set_error(VIE_ERR_BREAKDOWN, "BiCG breakdown at step " + std::to_string(m));
-        }
-        if (err < thr) {
-            if (verbose) printf("CG Error: %lf\nSteps: %d\n\n", err, m);
-            res.steps = m;
-            return VIE_OK;
-        }
-        if (verbose) printf("CG Error: %lf\n", err);
-    }
-    res.status = VIE_ERR_MAXIT;
-    return VIE_OK;
+        if ((rc2 = lin(ctx, LinArgs<C, 1, 0>{x, 1, {{p, cs(S_ALPHA)}}, {}}))) return rc2;
+        if ((rc2 = lin(ctx, LinArgs<C, 1, 1>{r, 1, {{Ap, cs(S_ALPHA, -1.0)}}, {{nullptr, 0}}}))) return rc2;
+        if ((rc2 = finalize<1>(ctx, kVecBlocks, FinBicgBeta{}))) return rc2;
+        // p += beta r (:489-491); then the stop rule (:497-505)
+        if ((rc2 = lin(ctx, LinArgs<C, 1, 0>{p, 1, {{r, cs(S_BETA)}}, {}}))) return rc2;
+        return finalize<1>(ctx, 1, then(FinNone{}, DecideErr{ctl, hist}));
+    };
+    rc = run_loop(ctx, body);
+    ctx->gate = Gate{nullptr, 0};
+    if (rc) return rc;
+    return finish(ctx, res, 0, 1, PS_ERR_STEPS, verbose, "BiCG");
 }
 
 template <typename T>
@@ -909,7 +1226,9 @@ static int true_residual(vie_ctx* ctx, const double2* b, const double2* x, doubl
 // the FP64 solution, r = b - A x is recomputed with the FP64 operator, and that
 // true residual replaces the FP32 one (rho and beta follow it).  The Krylov
 // directions p, v are kept, so no subspace is lost as in a restart.  The solve
-// stops only on the FP64 true residual.
+// stops only on the FP64 true residual.  The three phases (FP32 step, FP64
+// update, residual replacement) are gated on the control state, so one
+// captured body covers all of them.
 static int solve_bicgstab_mixed(vie_ctx* ctx, const double2* b64, double2* x64, double tol, double delta,
                                 int maxit, int verbose, KrylovResult& res, int& updates, int& mv64) {
     using C = float2;
@@ -928,76 +1247,63 @@ static int solve_bicgstab_mixed(vie_ctx* ctx, const double2* b64, double2* x64, 
     cudaStream_t st = ctx->stream;
     VIE_CUDA_TRY(cudaMemsetAsync(ctx->d_scal, 0, sizeof(double2) * S_COUNT, st), ctx->err);
     VIE_CUDA_TRY(cudaMemsetAsync(x64, 0, sizeof(double2) * n, st), ctx->err);
-    VIE_CUDA_TRY(cudaMemsetAsync(x32, 0, sizeof(C) * n, st), ctx->err);
-    k_to_f32<<<kVecBlocks, 256, 0, st>>>(b32, b64, n);
+    if ((rc = zero_vecs(ctx, sizeof(C) * n, {x32, p, v}))) return rc;
+    k_to_f32<<<kVecBlocks, 256, 0, st>>>(b32, b64, n, Gate{nullptr, 0});
     count_launch();
     VIE_CUDA_TRY(cudaMemcpyAsync(r, b32, sizeof(C) * n, cudaMemcpyDeviceToDevice, st), ctx->err);
+    if ((rc = ctl_init(ctx, tol, maxit, delta))) return rc;
+    KCtl* ctl = ctx->d_ctl;
+    double2* hist = ctx->d_hist;
     {
         // ||b||^2 from the FP64 right-hand side, rho = b^H r in FP32 data
         DotArgs<double2, 1> g{{b64}, {b64}, {1}};
         if ((rc = dots(ctx, g))) return rc;
-        if ((rc = finalize<1>(ctx, kVecBlocks, FinNorm{S_T5}))) return rc;
+        if ((rc = finalize<1>(ctx, kVecBlocks, FinCtlBn2{ctl}))) return rc;
         DotArgs<C, 2> g2{{b32, b32}, {b32, r}, {1, 1}};
         if ((rc = dots(ctx, g2))) return rc;
         if ((rc = finalize<2>(ctx, kVecBlocks, FinBicgstabInit{}))) return rc;
-        if ((rc = read_scalars(ctx))) return rc;
     }
-    const double bn2 = ctx->h_scal[S_T5].x;
-    double rmax2 = bn2;
     const long long nblk = epilogue_blocks(op);
-    for (int m = 0; m < maxit; m++) {
-        if (m == 0) {
-            if ((rc = opmv(ctx, op, ProCopyWrite<C>{r, p, a}, EpiDotB<C>{v, b32, a}, p, false))) return rc;
-        } else {
-            if ((rc = opmv(ctx, op, ProBicgP<C>{r, p, v, ctx->d_scal, a}, EpiDotB<C>{v, b32, a}, p, false))) return rc;
-        }
-        if ((rc = finalize<1>(ctx, nblk, FinAlpha{}))) return rc;
-        if ((rc = opmv(ctx, op, ProBicgS<C>{r, v, sv, ctx->d_scal, a}, EpiDotTS<C>{t, sv, a}, sv, false))) return rc;
-        if ((rc = finalize<2>(ctx, nblk, FinOmega{}))) return rc;
-        k_bicgstab_update<C><<<kVecBlocks, 256, 0, st>>>(x32, p, sv, t, r, b32, n, ctx->d_scal, ctx->d_partial);
+    const long long nblk64 = epilogue_blocks(ctx->op64);
+    auto body = [&]() -> int {
+        int rc2;
+        // FP32 BiCGSTAB step
+        ctx->gate = Gate{&ctl->state, KS_RUN};
+        if ((rc2 = opmv(ctx, op, ProBicgP<C>{r, p, v, ctx->d_scal, a}, EpiDotB<C>{v, b32, a}, p, false))) return rc2;
+        if ((rc2 = finalize<1>(ctx, nblk, FinAlpha{}))) return rc2;
+        if ((rc2 = opmv(ctx, op, ProBicgS<C>{r, v, sv, ctx->d_scal, a}, EpiDotTS<C>{t, sv, a}, sv, false))) return rc2;
+        if ((rc2 = finalize<2>(ctx, nblk, FinOmega{}))) return rc2;
+        k_bicgstab_update<C><<<kVecBlocks, 256, 0, ctx->stream>>>(x32, p, sv, t, r, b32, n, ctx->d_scal,
+                                                                   ctx->d_partial, ctx->gate);
         count_launch();
         VIE_CUDA_TRY(cudaGetLastError(), ctx->err);
-        if ((rc = finalize<2>(ctx, kVecBlocks, FinBicgstabUpdate{}))) return rc;
-        res.matvecs += 2;
-        res.iterations = m + 1;
-        if ((rc = read_scalars(ctx))) return rc;
-        const double rr = ctx->h_scal[S_RR].x;
-        double err = std::sqrt(rr / bn2);
-        res.err = err;
-        if (ctx->h_scal[S_NAN].x != 0.0 && !(err < tol)) {
-            res.status = VIE_ERR_BREAKDOWN;
-            return ctx->set_error(VIE_ERR_BREAKDOWN, "mixed BiCGSTAB breakdown at step " + std::to_string(m));
-        }
-        if (rr < delta * delta * rmax2 || err < tol) {
-            // reliable update: x += x32 in FP64, r = b - A x in FP64, r32 = float(r)
-            k_fold_correction<<<kVecBlocks, 256, 0, st>>>(x64, x32, n);
-            count_launch();
-            VIE_CUDA_TRY(cudaGetLastError(), ctx->err);
-            double rel;
-            double2 bnv = make_double2(bn2, 0.0);
-            if ((rc = true_residual(ctx, b64, x64, r64, &rel, &bnv))) return rc;
-            updates++;
-            mv64++;
-            err = rel;
-            res.err = rel;
-            if (verbose) printf("CG Error: %lf (true residual)\n", rel);
-            if (rel < tol) {
-                res.steps = m;
-                return VIE_OK;
-            }
-            k_to_f32<<<kVecBlocks, 256, 0, st>>>(r, r64, n);
-            count_launch();
-            DotArgs<C, 1> g{{b32}, {r}, {1}};
-            if ((rc = dots(ctx, g))) return rc;
-            if ((rc = finalize<1>(ctx, kVecBlocks, FinRhoReset{}))) return rc;
-            rmax2 = rel * rel * bn2;
-        } else {
-            rmax2 = std::max(rmax2, rr);
-            if (verbose) printf("CG Error: %lf\n", err);
-        }
-    }
-    res.status = VIE_ERR_MAXIT;
-    return VIE_OK;
+        if ((rc2 = finalize<2>(ctx, kVecBlocks, then(FinBicgstabUpdate{}, DecideReliable{ctl, hist})))) return rc2;
+        // reliable update (only when requested): x += x32 in FP64, r64 = b - A x in FP64
+        if ((rc2 = cond_begin(ctx, KS_UPDATE))) return rc2;
+        ctx->gate = Gate{&ctl->state, KS_UPDATE};
+        k_fold_correction<<<kVecBlocks, 256, 0, ctx->stream>>>(x64, x32, n, ctx->gate);
+        count_launch();
+        VIE_CUDA_TRY(cudaGetLastError(), ctx->err);
+        if ((rc2 = opmv(ctx, ctx->op64, ProCopy<double2>{x64, a}, EpiResidual<double2>{r64, b64, a}, x64, false)))
+            return rc2;
+        if ((rc2 = finalize<1>(ctx, nblk64, then(FinNorm{S_T5}, DecideTrue{ctl, hist})))) return rc2;
+        // residual replacement: r32 = float(r64); rho = b^H r and the next beta
+        ctx->gate = Gate{&ctl->state, KS_RESET};
+        k_to_f32<<<kVecBlocks, 256, 0, ctx->stream>>>(r, r64, n, ctx->gate);
+        count_launch();
+        VIE_CUDA_TRY(cudaGetLastError(), ctx->err);
+        DotArgs<C, 1> g{{b32}, {r}, {1}};
+        if ((rc2 = dots(ctx, g))) return rc2;
+        if ((rc2 = finalize<1>(ctx, kVecBlocks, then(FinRhoReset{}, DecideResume{ctl})))) return rc2;
+        return cond_end(ctx);
+    };
+    rc = run_loop(ctx, body);
+    ctx->gate = Gate{nullptr, 0};
+    if (rc) return rc;
+    rc = finish(ctx, res, 0, 2, PS_RELIABLE, verbose, "mixed BiCGSTAB");
+    updates = ctx->h_ctl->updates;
+    mv64 = updates;
+    return rc;
 }
 
 int solve_driver(vie_ctx* ctx, const vie_solve_params* prm, vie_solve_info* info) {
@@ -1012,6 +1318,7 @@ int solve_driver(vie_ctx* ctx, const vie_solve_params* prm, vie_solve_info* info
     VIE_CUDA_TRY(cudaEventRecord(e0, st), ctx->err);
     vie_solve_info out{};
     out.steps = -1;
+    const long long graphs0 = ctx->graph_launches;
     // masked right-hand side b (FP64) in work slot 20
     double2* b64 = (double2*)work_vec(ctx, 20, sizeof(double2), &rc);
     if (rc) return rc;
@@ -1119,6 +1426,7 @@ int solve_driver(vie_ctx* ctx, const vie_solve_params* prm, vie_solve_info* info
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     out.seconds = ms * 1e-3;
+    out.graph_loops = (int)(ctx->graph_launches - graphs0);
     // true residual in FP64 (after the timed region): the mixed loop already
     // holds it; an FP64 solve evaluates it on request
     if (prm->precision == VIE_PREC_MIXED) {

@@ -41,6 +41,16 @@ template <typename C> struct AxisTables {
     const int* gfold;          // slot -> folded index into the Green octant, [0, N]
 };
 
+// Device-side control of an iterative solve.  Every kernel of a captured
+// iteration carries a gate and returns at once unless the solve's state word
+// equals the state the kernel belongs to, so one iteration body can be
+// replayed (CUDA graph) without host decisions in between.
+struct Gate {
+    const int* state;  // nullptr: always open
+    int when;
+};
+__device__ __forceinline__ bool gate_closed(const Gate& g) { return g.state != nullptr && *g.state != g.when; }
+
 template <typename C> struct OpDev {
     int nx, ny, nz;
     long long a;               // nx*ny*nz
@@ -56,6 +66,7 @@ template <typename C> struct OpDev {
     typename real_of<C>::type dcoef[3];   // -delta_f Z0 / (2 k0)
     C* b;                      // 3 * nx*ny*2nz scratch
     C* c;                      // 3 * nx*2ny*2nz scratch
+    Gate gate;                 // launch gate of the current solve (state == nullptr: always run)
 };
 
 __host__ __device__ inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
@@ -115,6 +126,7 @@ __device__ __forceinline__ void block_reduce_store(double2 (&acc)[K], double2* _
 // ---------------------------------------------------------------------------
 template <typename C, class Pro>
 __global__ void __launch_bounds__(kThreads) k_fwd_z(OpDev<C> op, Pro pro) {
+    if (gate_closed(op.gate)) return;
     const int N = op.nz, T = op.tz, TP = T + 1;
     C* tw; unsigned short* perm; C* buf;
     load_axis_tables(op.ax[2], N, tw, perm, buf);
@@ -149,6 +161,7 @@ __global__ void __launch_bounds__(kThreads) k_fwd_z(OpDev<C> op, Pro pro) {
 // F2: forward y.  grid (kz tiles, nx, 3)
 template <typename C>
 __global__ void __launch_bounds__(kThreads) k_fwd_y(OpDev<C> op) {
+    if (gate_closed(op.gate)) return;
     const int N = op.ny, T = op.tc, TP = T;
     C* tw; unsigned short* perm; C* buf;
     load_axis_tables(op.ax[1], N, tw, perm, buf);
@@ -179,6 +192,7 @@ __global__ void __launch_bounds__(kThreads) k_fwd_y(OpDev<C> op) {
 // F3: forward x, spectral multiply, inverse x, crop.  grid (kz tiles, 2ny)
 template <typename C, bool CONJ>
 __global__ void __launch_bounds__(kThreads) k_x_spectral(OpDev<C> op) {
+    if (gate_closed(op.gate)) return;
     using R = typename real_of<C>::type;
     const int N = op.nx, T = op.tx, TP = T;
     C* tw; unsigned short* perm; C* buf;
@@ -234,6 +248,7 @@ __global__ void __launch_bounds__(kThreads) k_x_spectral(OpDev<C> op) {
 // I2: inverse y, crop.  grid (kz tiles, nx, 3)
 template <typename C>
 __global__ void __launch_bounds__(kThreads) k_inv_y(OpDev<C> op) {
+    if (gate_closed(op.gate)) return;
     const int N = op.ny, T = op.tc, TP = T;
     C* tw; unsigned short* perm; C* buf;
     load_axis_tables(op.ax[1], N, tw, perm, buf);
@@ -267,6 +282,7 @@ __global__ void __launch_bounds__(kThreads) k_inv_y(OpDev<C> op) {
 template <typename C, bool CONJ, class Epi>
 __global__ void __launch_bounds__(kThreads) k_inv_z(OpDev<C> op, const C* __restrict__ xin, Epi epi,
                                                      double2* __restrict__ partial) {
+    if (gate_closed(op.gate)) return;
     using R = typename real_of<C>::type;
     const int N = op.nz, T = op.tz, TP = T + 1;
     C* tw; unsigned short* perm; C* buf;
