@@ -156,12 +156,25 @@ typedef struct {
     double seconds;     /* device time of the solve */
     int graph_loops;    /* iteration loops of the solve that ran as one CUDA graph launch (a device-side
                            WHILE loop over the captured iteration body); 0: iterated from the host */
+    int status;         /* this solve's own status (VIE_OK, VIE_ERR_MAXIT, VIE_ERR_BREAKDOWN, ...) */
 } vie_solve_info;
 
 /* Solve A x = b for the current right-hand side from x0 = 0.  Replaces
    FFT_Program (CG_Iteration.h:1365-1388) and the driver it dispatches to.
    x (3a complex) may be NULL; the solution also stays on the device. */
 VIE_API int vie_solve(vie_ctx* ctx, const vie_solve_params* p, double* x, vie_solve_info* info);
+/* Batched solve (no reference counterpart: the reference runs one wavelength
+   per process, main.cpp:27-36).  Solves the systems of n distinct contexts on
+   the same GPU (each with its own grid, material, Green's function and
+   right-hand side: wavelength x polarisation sweeps, uneven particle grids) in
+   ONE CUDA graph launch: a device-side WHILE loop whose every pass runs each
+   still-unconverged instance's iteration body as a parallel branch; converged
+   instances launch nothing.  Same parameters for all instances; precision FP64
+   with any solver, or VIE_PREC_MIXED with BiCGSTAB.  Solutions stay in the
+   contexts (vie_get_solution); infos (n entries, may be NULL) receive each
+   instance's counts, `seconds` being the time of the whole batch.  Returns
+   the first non-OK instance status (VIE_ERR_MAXIT if any instance hit its cap). */
+VIE_API int vie_solve_batch(vie_ctx* const* ctxs, int n, const vie_solve_params* p, vie_solve_info* infos);
 /* ||b - A x|| / ||b|| of the last solution for the current right-hand side,
    evaluated in FP64 (one operator application). */
 VIE_API int vie_residual(vie_ctx* ctx, double* relres);

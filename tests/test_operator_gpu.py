@@ -45,7 +45,11 @@ def test_small_cases_match_reference(idx):
         assert rel(c.matvec(x, conj=True), gold[f"ahx{idx}"]) < FP64_TOL
 
 
-@pytest.mark.parametrize("shape", [(24, 20, 16), (31, 17, 13), (48, 40, 56), (9, 7, 5), (2, 2, 2), (16, 3, 64)])
+# shapes cover the generic kernels (odd and prime lengths) and every length
+# with register four-step kernels: 16..256 powers of two and the mixed-radix
+# 24 (8x3), 40 (8x5), 48 (8x6), 56 (8x7), 72 (8x9), 80 (16x5), 88 (8x11), 96 (16x6)
+@pytest.mark.parametrize("shape", [(24, 20, 16), (31, 17, 13), (48, 40, 56), (9, 7, 5), (2, 2, 2), (16, 3, 64),
+                                   (72, 88, 16), (96, 24, 80), (32, 72, 40)])
 def test_matvec_fp64_matches_oracle(shape):
     rng = np.random.default_rng(sum(shape))
     d = (0.01, 0.012, 0.011)
@@ -67,7 +71,7 @@ def _torch():
     return torch
 
 
-@pytest.mark.parametrize("shape", [(24, 20, 16), (31, 17, 13)])
+@pytest.mark.parametrize("shape", [(24, 20, 16), (31, 17, 13), (48, 40, 56), (72, 88, 16), (96, 24, 80)])
 def test_matvec_fp32_matches_oracle(shape):
     torch = _torch()
     rng = np.random.default_rng(5)
@@ -86,6 +90,10 @@ def test_matvec_fp32_matches_oracle(shape):
         c.matvec_dev(xt.data_ptr(), yt.data_ptr(), conj=False, precision=V.PREC_MIXED)
         c.sync()
         assert rel(yt.cpu().numpy(), ref) < FP32_TOL
+        refh = O.matvec(g, O.green(g), table[mat], flags, x, True)
+        c.matvec_dev(xt.data_ptr(), yt.data_ptr(), conj=True, precision=V.PREC_MIXED)
+        c.sync()
+        assert rel(yt.cpu().numpy(), refh) < FP32_TOL
 
 
 def test_adjoint_and_symmetry_identities_full_size():

@@ -61,7 +61,8 @@ class VieSolveParams(ctypes.Structure):
 class VieSolveInfo(ctypes.Structure):
     _fields_ = [("steps", ctypes.c_int), ("iterations", ctypes.c_int), ("outer", ctypes.c_int),
                 ("matvecs_fp64", ctypes.c_int), ("matvecs_fp32", ctypes.c_int), ("relres", ctypes.c_double),
-                ("true_relres", ctypes.c_double), ("seconds", ctypes.c_double), ("graph_loops", ctypes.c_int)]
+                ("true_relres", ctypes.c_double), ("seconds", ctypes.c_double), ("graph_loops", ctypes.c_int),
+                ("status", ctypes.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -101,6 +102,7 @@ def lib():
         L.vie_reset.argtypes = [_vp, _dp, ctypes.c_int]
         L.vie_matvec_dev.argtypes = [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int]
         L.vie_solve.argtypes = [_vp, P(VieSolveParams), _dp, P(VieSolveInfo)]
+        L.vie_solve_batch.argtypes = [P(_vp), ctypes.c_int, P(VieSolveParams), P(VieSolveInfo)]
         L.vie_get_solution.argtypes = [_vp, _dp]
         L.vie_residual.argtypes = [_vp, _dp]
         L.vie_solution_device.argtypes = [_vp, P(_vp)]
@@ -270,6 +272,33 @@ class Context:
 
     def sync(self):
         self._check(self._L.vie_sync(self._h))
+
+
+def solve_batch(contexts, solver="bicgstab", tol=1e-3, precision=PREC_FP64, max_iter=0, inner_tol=0.0,
+                verbose=False, copy=True, allow_maxit=False, raise_errors=True):
+    """Solve every context's system in one CUDA graph launch (``vie_solve_batch``).
+
+    The contexts may have different grids, materials, wavelengths and
+    right-hand sides; they must be distinct and on one GPU.  Returns one
+    SolveResult per context (``x`` copied back when ``copy``; ``status`` the
+    instance's own).  With ``raise_errors=False`` instance failures (cap,
+    breakdown) are only reported in the results."""
+    ctxs = list(contexts)
+    n = len(ctxs)
+    if n == 0:
+        return []
+    L = ctxs[0]._L
+    prm = VieSolveParams(SOLVERS[solver] if isinstance(solver, str) else int(solver), int(precision), float(tol),
+                         int(max_iter), float(inner_tol), 0, int(bool(verbose)), 0)
+    infos = (VieSolveInfo * n)()
+    handles = (_vp * n)(*[c._h for c in ctxs])
+    rc = L.vie_solve_batch(handles, n, ctypes.byref(prm), infos)
+    instance_failure = rc in (VIE_ERR_MAXIT, VIE_ERR_BREAKDOWN) and any(infos[i].status for i in range(n))
+    if rc != VIE_OK and not (instance_failure and not raise_errors) and not (rc == VIE_ERR_MAXIT and allow_maxit):
+        bad = next((c for c in ctxs if L.vie_last_error(c._h)), ctxs[0])
+        raise VieError(rc, L.vie_last_error(bad._h).decode(errors="replace"))
+    return [SolveResult(c.solution() if copy else None, infos[i].as_dict(), int(infos[i].status))
+            for i, c in enumerate(ctxs)]
 
 
 def launch_count() -> int:

@@ -13,6 +13,7 @@ int green_compute(vie_ctx* ctx);
 int green_expand(vie_ctx* ctx, double2* d_out);
 int incident_compute(vie_ctx* ctx, double theta, double phi, double psi, double2* d_e);
 int solve_driver(vie_ctx* ctx, const vie_solve_params* prm, vie_solve_info* info);
+int solve_batch_driver(vie_ctx* const* ctxs, int n, const vie_solve_params* prm, vie_solve_info* infos);
 int residual_driver(vie_ctx* ctx, double* relres);
 void mask_component(double2* v, const unsigned char* flags, long long a, int comp, cudaStream_t st);
 }  // namespace vie
@@ -338,6 +339,25 @@ int vie_solve(vie_ctx* ctx, const vie_solve_params* p, double* x, vie_solve_info
         if (e != cudaSuccess && !rc) rc = ctx->set_error(VIE_ERR_CUDA, cudaGetErrorString(e));
     }
     return rc;
+}
+
+int vie_solve_batch(vie_ctx* const* ctxs, int n, const vie_solve_params* p, vie_solve_info* infos) {
+    if (!ctxs || n < 1 || !p) return VIE_ERR_ARG;
+    for (int i = 0; i < n; i++) {
+        vie_ctx* c = ctxs[i];
+        if (check_ctx(c)) return VIE_ERR_ARG;
+        for (int k = 0; k < i; k++)
+            if (ctxs[k] == c) return c->set_error(VIE_ERR_ARG, "a context appears twice in the batch");
+        if (c->device != ctxs[0]->device) return c->set_error(VIE_ERR_ARG, "batch contexts on different devices");
+        int rc = ready_for_operator(c);
+        if (rc) return rc;
+        if (!c->have_rhs) return c->set_error(VIE_ERR_STATE, "no right-hand side (vie_incident / vie_set_rhs)");
+        c->err.code = VIE_OK;
+        c->err.msg.clear();
+    }
+    if (!(p->tol > 0)) return ctxs[0]->set_error(VIE_ERR_ARG, "tolerance must be positive");
+    cudaSetDevice(ctxs[0]->device);
+    return solve_batch_driver(ctxs, n, p, infos);
 }
 
 int vie_residual(vie_ctx* ctx, double* relres) {

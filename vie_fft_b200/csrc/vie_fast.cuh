@@ -23,21 +23,33 @@
 namespace vie {
 
 template <int N> struct FastPlan { static constexpr bool ok = false; static constexpr int R1 = 1, R2 = 1; };
-template <> struct FastPlan<256> { static constexpr bool ok = true; static constexpr int R1 = 16, R2 = 16; };
-template <> struct FastPlan<128> { static constexpr bool ok = true; static constexpr int R1 = 16, R2 = 8; };
-template <> struct FastPlan<64> { static constexpr bool ok = true; static constexpr int R1 = 8, R2 = 8; };
-template <> struct FastPlan<32> { static constexpr bool ok = true; static constexpr int R1 = 8, R2 = 4; };
-template <> struct FastPlan<16> { static constexpr bool ok = true; static constexpr int R1 = 4, R2 = 4; };
+#define VIE_FAST_PLAN(NN, A, B) \
+    template <> struct FastPlan<NN> { static constexpr bool ok = true; static constexpr int R1 = A, R2 = B; };
+VIE_FAST_PLAN(256, 16, 16)
+VIE_FAST_PLAN(128, 16, 8)
+VIE_FAST_PLAN(96, 16, 6)
+VIE_FAST_PLAN(88, 8, 11)
+VIE_FAST_PLAN(80, 16, 5)
+VIE_FAST_PLAN(72, 8, 9)
+VIE_FAST_PLAN(64, 8, 8)
+VIE_FAST_PLAN(56, 8, 7)
+VIE_FAST_PLAN(48, 8, 6)
+VIE_FAST_PLAN(40, 8, 5)
+VIE_FAST_PLAN(32, 8, 4)
+VIE_FAST_PLAN(24, 8, 3)
+VIE_FAST_PLAN(16, 4, 4)
+#undef VIE_FAST_PLAN
+// the axis lengths with register four-step kernels (one case per FastPlan above)
+#define VIE_FAST_LENGTHS(X) X(256) X(128) X(96) X(88) X(80) X(72) X(64) X(56) X(48) X(40) X(32) X(24) X(16)
 
-inline bool fast_length(int n) { return n == 256 || n == 128 || n == 64 || n == 32 || n == 16; }
-
-template <int R, bool INV, typename C> __device__ __forceinline__ void dft_reg(C* v) {
-    if constexpr (R == 2) dft2<INV>(v[0], v[1]);
-    else if constexpr (R == 4) dft4<INV>(v[0], v[1], v[2], v[3]);
-    else if constexpr (R == 8) dft8<INV>(v);
-    else if constexpr (R == 16) dft16<INV>(v);
-    else static_assert(R == 2, "unsupported register radix");
+inline bool fast_length(int n) {
+#define VIE_FL_CASE(NN) if (n == NN) return true;
+    VIE_FAST_LENGTHS(VIE_FL_CASE)
+#undef VIE_FL_CASE
+    return false;
 }
+
+template <int R, bool INV, typename C> __device__ __forceinline__ void dft_reg(C* v) { dft_reg_any<R, INV>(v); }
 
 // pencils per CTA of the column passes (one row segment of TP * sizeof(C) bytes)
 template <typename C> struct FastTiles;

@@ -16,6 +16,7 @@
 // (the half-length twiddles exp(-2 pi i t / N) are tw[2t]); the same table
 // provides the exp(-2 pi i n / 2N) factors of the zero-padding split.
 #pragma once
+#include <type_traits>
 #include "vie_complex.cuh"
 
 namespace vie {
@@ -137,6 +138,135 @@ template <bool INV, typename C> __host__ __device__ __forceinline__ void dft5(C*
     v[4] = csub(p1, q1);
     v[2] = cadd(p2, q2);
     v[3] = csub(p2, q2);
+}
+
+// ---------------------------------------------------------------------------
+// compile-time twiddles W_R^e = exp(-2 pi i e / R) for the register codelets
+// of radices 6, 7, 9, 10, 11, 12.  cos/sin come from Taylor series evaluated
+// by the compiler after reduction of the angle to |r| <= pi/4 around the
+// nearest quarter turn (exact integer reduction; 12 terms leave < 1e-20).
+// ---------------------------------------------------------------------------
+struct CtCS {
+    double c, s;
+};
+__host__ __device__ constexpr CtCS ct_cos_sin_2pi(long long p, long long q) {
+    constexpr double two_pi = 6.283185307179586476925286766559;
+    p %= q;
+    if (p < 0) p += q;
+    const long long k = (4 * p + q / 2) / q;             // nearest quarter turn
+    const double r = two_pi * (double)(4 * p - k * q) / (double)(4 * q);
+    double sn = r, cs = 1.0, ts = r, tc = 1.0;
+    for (int n = 1; n < 12; n++) {
+        ts *= -r * r / (double)((2 * n) * (2 * n + 1));
+        tc *= -r * r / (double)((2 * n - 1) * (2 * n));
+        sn += ts;
+        cs += tc;
+    }
+    switch (k & 3) {
+        case 0: return CtCS{cs, sn};
+        case 1: return CtCS{-sn, cs};
+        case 2: return CtCS{-cs, -sn};
+        default: return CtCS{sn, -cs};
+    }
+}
+template <int E, int R> struct CtW {
+    static constexpr CtCS v = ct_cos_sin_2pi(E, R);
+    static constexpr double c = v.c, s = v.s;   // W_R^E = c - i s
+};
+
+template <int B, int E, class F> __host__ __device__ __forceinline__ void static_for(F&& f) {
+    if constexpr (B < E) {
+        f(std::integral_constant<int, B>{});
+        static_for<B + 1, E>(f);
+    }
+}
+
+// x * W_R^E (forward) or x * conj(W_R^E) (inverse)
+template <int R, int E, bool INV, typename C> __host__ __device__ __forceinline__ C ct_twiddle(C x) {
+    using Rl = typename real_of<C>::type;
+    constexpr int e = ((E % R) + R) % R;
+    if constexpr (e == 0) {
+        return x;
+    } else {
+        constexpr double c = CtW<e, R>::c, sn = INV ? -CtW<e, R>::s : CtW<e, R>::s;
+        // (c - i sn) x
+        return mkc((Rl)c * x.x + (Rl)sn * x.y, (Rl)c * x.y - (Rl)sn * x.x);
+    }
+}
+
+template <int R, bool INV, typename C> __host__ __device__ __forceinline__ void dft_reg_any(C* v);
+
+// odd R: pairs r, R-r folded, X_k = x0 + sum a_r cos - i sum b_r sin (forward)
+template <int R, bool INV, typename C> __host__ __device__ __forceinline__ void dft_odd(C* v) {
+    using Rl = typename real_of<C>::type;
+    constexpr int H = (R - 1) / 2;
+    C a[H], b[H];
+    const C x0 = v[0];
+    C sum = x0;
+#pragma unroll
+    for (int j = 0; j < H; j++) {
+        a[j] = cadd(v[j + 1], v[R - 1 - j]);
+        b[j] = csub(v[j + 1], v[R - 1 - j]);
+        sum = cadd(sum, a[j]);
+    }
+    v[0] = sum;
+    static_for<1, H + 1>([&](auto kc) {
+        constexpr int k = decltype(kc)::value;
+        C re = x0, im = czero<C>();
+        static_for<0, H>([&](auto jc) {
+            constexpr int j = decltype(jc)::value;
+            constexpr int e = ((j + 1) * k) % R;
+            re = cadd(re, cscale(a[j], (Rl)CtW<e, R>::c));
+            im = cadd(im, cscale(b[j], (Rl)CtW<e, R>::s));
+        });
+        const C jim = INV ? cmul_pi(im) : cmul_mi(im);
+        v[k] = cadd(re, jim);
+        v[R - k] = csub(re, jim);
+    });
+}
+
+// R = P Q in registers: DFT_P over stride-Q subsequences, twiddles W_R^{n2 k1},
+// DFT_Q; natural order in and out
+template <int P, int Q, bool INV, typename C> __host__ __device__ __forceinline__ void dft_pq(C* v) {
+    constexpr int R = P * Q;
+    C t[R];
+    static_for<0, Q>([&](auto n2c) {
+        constexpr int n2 = decltype(n2c)::value;
+        C u[P];
+#pragma unroll
+        for (int n1 = 0; n1 < P; n1++) u[n1] = v[n2 + Q * n1];
+        dft_reg_any<P, INV>(u);
+        static_for<0, P>([&](auto k1c) {
+            constexpr int k1 = decltype(k1c)::value;
+            t[n2 * P + k1] = ct_twiddle<R, n2 * k1, INV>(u[k1]);
+        });
+    });
+#pragma unroll
+    for (int k1 = 0; k1 < P; k1++) {
+        C w[Q];
+#pragma unroll
+        for (int n2 = 0; n2 < Q; n2++) w[n2] = t[n2 * P + k1];
+        dft_reg_any<Q, INV>(w);
+#pragma unroll
+        for (int k2 = 0; k2 < Q; k2++) v[k1 + P * k2] = w[k2];
+    }
+}
+
+// register DFT of a compile-time radix
+template <int R, bool INV, typename C> __host__ __device__ __forceinline__ void dft_reg_any(C* v) {
+    if constexpr (R == 1) {
+    } else if constexpr (R == 2) dft2<INV>(v[0], v[1]);
+    else if constexpr (R == 3) dft3<INV>(v);
+    else if constexpr (R == 4) dft4<INV>(v[0], v[1], v[2], v[3]);
+    else if constexpr (R == 5) dft5<INV>(v);
+    else if constexpr (R == 6) dft_pq<2, 3, INV>(v);
+    else if constexpr (R == 8) dft8<INV>(v);
+    else if constexpr (R == 9) dft_pq<3, 3, INV>(v);
+    else if constexpr (R == 10) dft_pq<2, 5, INV>(v);
+    else if constexpr (R == 12) dft_pq<4, 3, INV>(v);
+    else if constexpr (R == 16) dft16<INV>(v);
+    else if constexpr (R % 2 == 1) dft_odd<R, INV>(v);
+    else static_assert(R == 2, "unsupported register radix");
 }
 
 // direct O(R^2) DFT for any other radix; W_R^e = tw[2 e (N/R)] (tw has 2N entries)

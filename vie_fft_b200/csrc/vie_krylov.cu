@@ -21,6 +21,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <initializer_list>
 #include <string>
 #include <vector>
@@ -883,6 +884,156 @@ static int run_loop(vie_ctx* ctx, Body body) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// several solves in one graph loop
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool ks_live_dev(int s) { return s == KS_RUN || s == KS_UPDATE || s == KS_RESET; }
+
+// start of a batch pass: open the IF node of every instance that is still live
+__global__ void k_batch_live(KCtl* const* __restrict__ ctls, const cudaGraphConditionalHandle* __restrict__ hs, int n) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const bool live = ks_live_dev(ctls[i]->state);
+        if (live) ctls[i]->loops++;
+        cudaGraphSetConditional(hs[i], live ? 1u : 0u);
+    }
+}
+// end of a batch pass: loop again while any instance is live
+__global__ void k_batch_cond(KCtl* const* __restrict__ ctls, int n, cudaGraphConditionalHandle h, int* passes) {
+    int any = 0;
+    for (int i = threadIdx.x; i < n; i += 32) any |= ks_live_dev(ctls[i]->state) ? 1 : 0;
+    any = __any_sync(0xffffffffu, any);
+    if (threadIdx.x == 0) {
+        (*passes)++;
+        cudaGraphSetConditional(h, any ? 1u : 0u);
+    }
+}
+
+template <class PlanT>
+static int run_loop_batch_graph(std::vector<PlanT*>& plans, cudaStream_t S, vie_ctx* ectx, bool& launched) {
+    const int n = (int)plans.size();
+    launched = false;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    void* dmem = nullptr;
+    int rc = VIE_OK;
+    std::vector<long long> per(n, 0);
+    do {
+        // device arrays: control-block pointers, IF handles, pass counter
+        const size_t off_h = align_up(sizeof(KCtl*) * n, 64), off_p = align_up(off_h + sizeof(cudaGraphConditionalHandle) * n, 64);
+        if (cudaMalloc(&dmem, off_p + 64) != cudaSuccess) { rc = ectx->set_error(VIE_ERR_ALLOC, "batch control arrays"); break; }
+        KCtl** d_ctls = (KCtl**)dmem;
+        cudaGraphConditionalHandle* d_hs = (cudaGraphConditionalHandle*)((char*)dmem + off_h);
+        int* d_passes = (int*)((char*)dmem + off_p);
+        cudaGraphConditionalHandle hw;
+        if (cudaGraphCreate(&graph, 0) != cudaSuccess ||
+            cudaGraphConditionalHandleCreate(&hw, graph, 1, cudaGraphCondAssignDefault) != cudaSuccess) {
+            rc = ectx->set_error(VIE_ERR_CUDA, "batch graph / WHILE handle");
+            break;
+        }
+        cudaGraphNodeParams wp = {cudaGraphNodeTypeConditional};
+        wp.conditional.handle = hw;
+        wp.conditional.type = cudaGraphCondTypeWhile;
+        wp.conditional.size = 1;
+        cudaGraphNode_t wnode;
+        if (cudaGraphAddNode(&wnode, graph, nullptr, 0, &wp) != cudaSuccess) {
+            rc = ectx->set_error(VIE_ERR_CUDA, "batch WHILE node");
+            break;
+        }
+        cudaGraph_t bodyg = wp.conditional.phGraph_out[0];
+        std::vector<cudaGraphConditionalHandle> hs(n);
+        std::vector<KCtl*> ctls(n);
+        bool ok = true;
+        for (int i = 0; i < n && ok; i++) {
+            ok = cudaGraphConditionalHandleCreate(&hs[i], bodyg, 0, cudaGraphCondAssignDefault) == cudaSuccess;
+            ctls[i] = plans[i]->ctx->d_ctl;
+        }
+        if (!ok || cudaMemcpy(d_ctls, ctls.data(), sizeof(KCtl*) * n, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(d_hs, hs.data(), sizeof(cudaGraphConditionalHandle) * n, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemset(d_passes, 0, sizeof(int)) != cudaSuccess) {
+            rc = ectx->set_error(VIE_ERR_CUDA, "batch IF handles");
+            break;
+        }
+        if (cudaStreamBeginCaptureToGraph(S, bodyg, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) != cudaSuccess) {
+            rc = ectx->set_error(VIE_ERR_CUDA, "stream capture of the batch body");
+            break;
+        }
+        k_batch_live<<<1, 256, 0, S>>>(d_ctls, d_hs, n);
+        cudaStreamCaptureStatus cst;
+        cudaGraph_t g2 = nullptr;
+        const cudaGraphNode_t* dp = nullptr;
+        size_t nd = 0;
+        std::vector<cudaGraphNode_t> deps, ifs(n);
+        if (cudaStreamGetCaptureInfo(S, &cst, nullptr, &g2, &dp, &nd) == cudaSuccess) deps.assign(dp, dp + nd);
+        else ok = false;
+        for (int i = 0; i < n && ok && !rc; i++) {
+            vie_ctx* c = plans[i]->ctx;
+            cudaGraphNodeParams ip = {cudaGraphNodeTypeConditional};
+            ip.conditional.handle = hs[i];
+            ip.conditional.type = cudaGraphCondTypeIf;
+            ip.conditional.size = 1;
+            if (cudaGraphAddNode(&ifs[i], bodyg, deps.data(), deps.size(), &ip) != cudaSuccess ||
+                cudaStreamBeginCaptureToGraph(c->stream, ip.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                              cudaStreamCaptureModeRelaxed) != cudaSuccess) {
+                ok = false;
+                break;
+            }
+            const long long n0 = g_launches.load();
+            c->capturing = 1;
+            const int brc = plans[i]->body();
+            if (c->stream_parent) {
+                cudaGraph_t tmp = nullptr;
+                cudaStreamEndCapture(c->stream_aux, &tmp);
+                c->stream = c->stream_parent;
+                c->stream_parent = nullptr;
+            }
+            c->capturing = 0;
+            c->gate = Gate{nullptr, 0};
+            cudaGraph_t tmp = nullptr;
+            const cudaError_t ce = cudaStreamEndCapture(c->stream, &tmp);
+            per[i] = g_launches.load() - n0;
+            count_launch(-per[i]);
+            if (brc) rc = brc;
+            else if (ce != cudaSuccess) ok = false;
+        }
+        if (ok && !rc)
+            ok = cudaStreamUpdateCaptureDependencies(S, ifs.data(), n, cudaStreamSetCaptureDependencies) == cudaSuccess;
+        k_batch_cond<<<1, 32, 0, S>>>(d_ctls, n, hw, d_passes);
+        cudaGraph_t captured = nullptr;
+        const cudaError_t ce = cudaStreamEndCapture(S, &captured);
+        if (rc) break;
+        if (!ok || ce != cudaSuccess) {
+            rc = ectx->set_error(VIE_ERR_CUDA, "capture of the batch body");
+            break;
+        }
+        if (cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) {
+            rc = ectx->set_error(VIE_ERR_CUDA, "batch graph instantiation");
+            break;
+        }
+        launched = true;
+        if (cudaGraphLaunch(exec, S) != cudaSuccess || cudaStreamSynchronize(S) != cudaSuccess) {
+            rc = ectx->set_error(VIE_ERR_CUDA, std::string("batch graph: ") + cudaGetErrorString(cudaGetLastError()));
+            break;
+        }
+        int passes = 0;
+        if (cudaMemcpy(&passes, d_passes, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) {
+            rc = ectx->set_error(VIE_ERR_CUDA, "batch pass count");
+            break;
+        }
+        count_launch(2LL * passes);
+        for (int i = 0; i < n && !rc; i++) {
+            vie_ctx* c = plans[i]->ctx;
+            if ((rc = ctl_read(c))) break;
+            count_launch(per[i] * c->h_ctl->loops);
+            c->graph_launches++;
+        }
+    } while (0);
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (dmem) cudaFree(dmem);
+    if (rc && !launched) (void)cudaGetLastError();
+    return rc;
+}
+
 // the drivers' console output, replayed from the device history:
 // "CG Error" per step, "Steps" at convergence (CG_Iteration.h:323-331 etc.);
 // BiCORSTAB prints only "Steps" at convergence (:1315-1327); the mixed solve
@@ -932,6 +1083,29 @@ static int finish(vie_ctx* ctx, KrylovResult& res, int mv_setup, int mv_per_iter
                                                  std::to_string(c.iter - 1));
 }
 
+// A solve split into its set-up (already enqueued on the context stream), an
+// iteration body and a completion step, so that several solves can share one
+// graph loop (vie_solve_batch).
+struct SolvePlan {
+    vie_ctx* ctx = nullptr;
+    std::function<int()> body;
+    std::function<int()> finish;
+};
+
+// run the loop now (plan == nullptr) or hand body and completion to a batch
+static int launch_or_plan(vie_ctx* ctx, SolvePlan* plan, std::function<int()> body, std::function<int()> fin) {
+    if (plan) {
+        plan->ctx = ctx;
+        plan->body = std::move(body);
+        plan->finish = std::move(fin);
+        return VIE_OK;
+    }
+    int rc = run_loop(ctx, body);
+    ctx->gate = Gate{nullptr, 0};
+    if (rc) return rc;
+    return fin();
+}
+
 static int zero_vecs(vie_ctx* ctx, size_t bytes, std::initializer_list<void*> vs) {
     for (void* v : vs) VIE_CUDA_TRY(cudaMemsetAsync(v, 0, bytes, ctx->stream), ctx->err);
     return VIE_OK;
@@ -946,7 +1120,7 @@ static int zero_vecs(vie_ctx* ctx, size_t bytes, std::initializer_list<void*> vs
 // ---------------------------------------------------------------------------
 template <typename T>
 static int solve_bicgstab(vie_ctx* ctx, Operator<T>& op, const cplx_t<T>* b, cplx_t<T>* x, double thr, int maxit,
-                          int verbose, int vbase, KrylovResult& res) {
+                          int verbose, int vbase, KrylovResult& res, SolvePlan* plan = nullptr) {
     using C = cplx_t<T>;
     int rc = VIE_OK;
     const long long a = ctx->a, n = 3 * a;
@@ -968,7 +1142,7 @@ static int solve_bicgstab(vie_ctx* ctx, Operator<T>& op, const cplx_t<T>* b, cpl
     KCtl* ctl = ctx->d_ctl;
     double2* hist = ctx->d_hist;
     const long long nblk = epilogue_blocks(op);
-    auto body = [&]() -> int {
+    auto body = [=, &op]() -> int {
         int rc2;
         ctx->gate = Gate{&ctl->state, KS_RUN};
         // p = r + beta (p - omega v) (:611-633); v = A p; b^H v (:652-662)
@@ -977,20 +1151,19 @@ static int solve_bicgstab(vie_ctx* ctx, Operator<T>& op, const cplx_t<T>* b, cpl
         // s = r - alpha v (:664-672); t = A s; t^H s, t^H t (:689-706)
         if ((rc2 = opmv(ctx, op, ProBicgS<C>{r, v, sv, ctx->d_scal, a}, EpiDotTS<C>{t, sv, a}, sv, false))) return rc2;
         if ((rc2 = finalize<2>(ctx, nblk, FinOmega{}))) return rc2;
-        k_bicgstab_update<C><<<kVecBlocks, 256, 0, st>>>(x, p, sv, t, r, b, n, ctx->d_scal, ctx->d_partial, ctx->gate);
+        k_bicgstab_update<C><<<kVecBlocks, 256, 0, ctx->stream>>>(x, p, sv, t, r, b, n, ctx->d_scal, ctx->d_partial,
+                                                                   ctx->gate);
         count_launch();
         VIE_CUDA_TRY(cudaGetLastError(), ctx->err);
         return finalize<2>(ctx, kVecBlocks, then(FinBicgstabUpdate{}, DecideErr{ctl, hist}));
     };
-    rc = run_loop(ctx, body);
-    ctx->gate = Gate{nullptr, 0};
-    if (rc) return rc;
-    return finish(ctx, res, 0, 2, PS_ERR_STEPS, verbose, "BiCGSTAB");
+    auto fin = [ctx, &res, verbose]() { return finish(ctx, res, 0, 2, PS_ERR_STEPS, verbose, "BiCGSTAB"); };
+    return launch_or_plan(ctx, plan, body, fin);
 }
 
 template <typename T>
 static int solve_cors(vie_ctx* ctx, Operator<T>& op, const cplx_t<T>* b, cplx_t<T>* x, double thr, int maxit,
-                      int verbose, int vbase, KrylovResult& res) {
+                      int verbose, int vbase, KrylovResult& res, SolvePlan* plan = nullptr) {
     using C = cplx_t<T>;
     int rc = VIE_OK;
     const long long a = ctx->a, n = 3 * a;
@@ -1015,7 +1188,7 @@ static int solve_cors(vie_ctx* ctx, Operator<T>& op, const cplx_t<T>* b, cplx_t<
     KCtl* ctl = ctx->d_ctl;
     double2* hist = ctx->d_hist;
     const long long nblk = epilogue_blocks(op);
-    auto body = [&]() -> int {
+    auto body = [=, &op]() -> int {
         int rc2;
         ctx->gate = Gate{&ctl->state, KS_RUN};
         // Ap = A r; rho = b^H Ap (:853-869)
@@ -1038,15 +1211,13 @@ static int solve_cors(vie_ctx* ctx, Operator<T>& op, const cplx_t<T>* b, cplx_t<
             return rc2;
         return finalize<1>(ctx, kVecBlocks, then(FinErr{}, DecideErr{ctl, hist}));
     };
-    rc = run_loop(ctx, body);
-    ctx->gate = Gate{nullptr, 0};
-    if (rc) return rc;
-    return finish(ctx, res, 0, 2, PS_ERR_STEPS, verbose, "CORS");
+    auto fin = [ctx, &res, verbose]() { return finish(ctx, res, 0, 2, PS_ERR_STEPS, verbose, "CORS"); };
+    return launch_or_plan(ctx, plan, body, fin);
 }
 
 template <typename T>
 static int solve_bicorstab(vie_ctx* ctx, Operator<T>& op, const cplx_t<T>* b, cplx_t<T>* x, double thr, int maxit,
-                           int verbose, int vbase, KrylovResult& res) {
+                           int verbose, int vbase, KrylovResult& res, SolvePlan* plan = nullptr) {
     using C = cplx_t<T>;
     int rc = VIE_OK;
     const long long a = ctx->a, n = 3 * a;
@@ -1070,7 +1241,7 @@ static int solve_bicorstab(vie_ctx* ctx, Operator<T>& op, const cplx_t<T>* b, cp
     KCtl* ctl = ctx->d_ctl;
     double2* hist = ctx->d_hist;
     const long long nblk = epilogue_blocks(op);
-    auto body = [&]() -> int {
+    auto body = [=, &op]() -> int {
         int rc2;
         ctx->gate = Gate{&ctl->state, KS_RUN};
         if ((rc2 = opmv(ctx, op, ProCopy<C>{r, a}, EpiDotB<C>{Ap, b, a}, r, false))) return rc2;   // :1145-1162
@@ -1095,15 +1266,13 @@ static int solve_bicorstab(vie_ctx* ctx, Operator<T>& op, const cplx_t<T>* b, cp
             return rc2;
         return finalize<1>(ctx, kVecBlocks, then(FinErr{}, DecideErr{ctl, hist}));
     };
-    rc = run_loop(ctx, body);
-    ctx->gate = Gate{nullptr, 0};
-    if (rc) return rc;
-    return finish(ctx, res, 0, 2, PS_STEPS_ONLY, verbose, "BiCORSTAB");
+    auto fin = [ctx, &res, verbose]() { return finish(ctx, res, 0, 2, PS_STEPS_ONLY, verbose, "BiCORSTAB"); };
+    return launch_or_plan(ctx, plan, body, fin);
 }
 
 template <typename T>
 static int solve_cg(vie_ctx* ctx, Operator<T>& op, const cplx_t<T>* b, cplx_t<T>* x, double thr, int maxit,
-                    int verbose, int vbase, KrylovResult& res) {
+                    int verbose, int vbase, KrylovResult& res, SolvePlan* plan = nullptr) {
     using C = cplx_t<T>;
     int rc = VIE_OK;
     const long long a = ctx->a, n = 3 * a;
@@ -1126,7 +1295,7 @@ static int solve_cg(vie_ctx* ctx, Operator<T>& op, const cplx_t<T>* b, cplx_t<T>
     if ((rc = ctl_init(ctx, thr, maxit, 0.0))) return rc;
     KCtl* ctl = ctx->d_ctl;
     double2* hist = ctx->d_hist;
-    auto body = [&]() -> int {
+    auto body = [=, &op]() -> int {
         int rc2;
         ctx->gate = Gate{&ctl->state, KS_RUN};
         if ((rc2 = opmv(ctx, op, ProCopy<C>{p, a}, EpiNorm<C>{Ap, a}, p, false))) return rc2;  // :253-268
@@ -1142,15 +1311,13 @@ static int solve_cg(vie_ctx* ctx, Operator<T>& op, const cplx_t<T>* b, cplx_t<T>
         if ((rc2 = lin(ctx, LinArgs<C, 2, 0>{p, 0, {{p, cs(S_BETA)}, {q, cs(-1, -1.0)}}, {}}))) return rc2;
         return finalize<1>(ctx, 1, then(FinNone{}, DecideErr{ctl, hist}));
     };
-    rc = run_loop(ctx, body);
-    ctx->gate = Gate{nullptr, 0};
-    if (rc) return rc;
-    return finish(ctx, res, 1, 2, PS_ERR_STEPS, verbose, "CG");
+    auto fin = [ctx, &res, verbose]() { return finish(ctx, res, 1, 2, PS_ERR_STEPS, verbose, "CG"); };
+    return launch_or_plan(ctx, plan, body, fin);
 }
 
 template <typename T>
 static int solve_bicg(vie_ctx* ctx, Operator<T>& op, const cplx_t<T>* b, cplx_t<T>* x, double thr, int maxit,
-                      int verbose, int vbase, KrylovResult& res) {
+                      int verbose, int vbase, KrylovResult& res, SolvePlan* plan = nullptr) {
     using C = cplx_t<T>;
     int rc = VIE_OK;
     const long long a = ctx->a, n = 3 * a;
@@ -1172,7 +1339,7 @@ static int solve_bicg(vie_ctx* ctx, Operator<T>& op, const cplx_t<T>* b, cplx_t<
     KCtl* ctl = ctx->d_ctl;
     double2* hist = ctx->d_hist;
     const long long nblk = epilogue_blocks(op);
-    auto body = [&]() -> int {
+    auto body = [=, &op]() -> int {
         int rc2;
         ctx->gate = Gate{&ctl->state, KS_RUN};
         if ((rc2 = opmv(ctx, op, ProCopy<C>{p, a}, EpiDotU<C>{Ap, p, a}, p, false))) return rc2;  // :437-453
@@ -1185,22 +1352,20 @@ static int solve_bicg(vie_ctx* ctx, Operator<T>& op, const cplx_t<T>* b, cplx_t<
         if ((rc2 = lin(ctx, LinArgs<C, 1, 0>{p, 1, {{r, cs(S_BETA)}}, {}}))) return rc2;
         return finalize<1>(ctx, 1, then(FinNone{}, DecideErr{ctl, hist}));
     };
-    rc = run_loop(ctx, body);
-    ctx->gate = Gate{nullptr, 0};
-    if (rc) return rc;
-    return finish(ctx, res, 0, 1, PS_ERR_STEPS, verbose, "BiCG");
+    auto fin = [ctx, &res, verbose]() { return finish(ctx, res, 0, 1, PS_ERR_STEPS, verbose, "BiCG"); };
+    return launch_or_plan(ctx, plan, body, fin);
 }
 
 template <typename T>
 static int run_solver(vie_ctx* ctx, Operator<T>& op, int solver, const cplx_t<T>* b, cplx_t<T>* x, double thr,
-                      int maxit, int verbose, int vbase, KrylovResult& res) {
+                      int maxit, int verbose, int vbase, KrylovResult& res, SolvePlan* plan = nullptr) {
     VIE_CUDA_TRY(cudaMemsetAsync(ctx->d_scal, 0, sizeof(double2) * S_COUNT, ctx->stream), ctx->err);
     switch (solver) {
-        case VIE_SOLVER_BICGSTAB: return solve_bicgstab<T>(ctx, op, b, x, thr, maxit, verbose, vbase, res);
-        case VIE_SOLVER_CORS: return solve_cors<T>(ctx, op, b, x, thr, maxit, verbose, vbase, res);
-        case VIE_SOLVER_CG: return solve_cg<T>(ctx, op, b, x, thr, maxit, verbose, vbase, res);
-        case VIE_SOLVER_BICG: return solve_bicg<T>(ctx, op, b, x, thr, maxit, verbose, vbase, res);
-        case VIE_SOLVER_BICORSTAB: return solve_bicorstab<T>(ctx, op, b, x, thr, maxit, verbose, vbase, res);
+        case VIE_SOLVER_BICGSTAB: return solve_bicgstab<T>(ctx, op, b, x, thr, maxit, verbose, vbase, res, plan);
+        case VIE_SOLVER_CORS: return solve_cors<T>(ctx, op, b, x, thr, maxit, verbose, vbase, res, plan);
+        case VIE_SOLVER_CG: return solve_cg<T>(ctx, op, b, x, thr, maxit, verbose, vbase, res, plan);
+        case VIE_SOLVER_BICG: return solve_bicg<T>(ctx, op, b, x, thr, maxit, verbose, vbase, res, plan);
+        case VIE_SOLVER_BICORSTAB: return solve_bicorstab<T>(ctx, op, b, x, thr, maxit, verbose, vbase, res, plan);
         default: return ctx->set_error(VIE_ERR_ARG, "unknown solver " + std::to_string(solver));
     }
 }
@@ -1230,7 +1395,8 @@ static int true_residual(vie_ctx* ctx, const double2* b, const double2* x, doubl
 // update, residual replacement) are gated on the control state, so one
 // captured body covers all of them.
 static int solve_bicgstab_mixed(vie_ctx* ctx, const double2* b64, double2* x64, double tol, double delta,
-                                int maxit, int verbose, KrylovResult& res, int& updates, int& mv64) {
+                                int maxit, int verbose, KrylovResult& res, int& updates, int& mv64,
+                                SolvePlan* plan = nullptr) {
     using C = float2;
     int rc = VIE_OK;
     const long long a = ctx->a, n = 3 * a;
@@ -1265,7 +1431,7 @@ static int solve_bicgstab_mixed(vie_ctx* ctx, const double2* b64, double2* x64, 
     }
     const long long nblk = epilogue_blocks(op);
     const long long nblk64 = epilogue_blocks(ctx->op64);
-    auto body = [&]() -> int {
+    auto body = [=, &op]() -> int {
         int rc2;
         // FP32 BiCGSTAB step
         ctx->gate = Gate{&ctl->state, KS_RUN};
@@ -1297,13 +1463,32 @@ static int solve_bicgstab_mixed(vie_ctx* ctx, const double2* b64, double2* x64, 
         if ((rc2 = finalize<1>(ctx, kVecBlocks, then(FinRhoReset{}, DecideResume{ctl})))) return rc2;
         return cond_end(ctx);
     };
-    rc = run_loop(ctx, body);
-    ctx->gate = Gate{nullptr, 0};
+    auto fin = [ctx, &res, &updates, &mv64, verbose]() {
+        const int rc2 = finish(ctx, res, 0, 2, PS_RELIABLE, verbose, "mixed BiCGSTAB");
+        updates = ctx->h_ctl->updates;
+        mv64 = updates;
+        return rc2;
+    };
+    return launch_or_plan(ctx, plan, body, fin);
+}
+
+// masked FP64 right-hand side b = E_inc . Flag (work slot 20) and ||b||^2
+static int prepare_rhs(vie_ctx* ctx, double2** b64_out, double2* bn2_out) {
+    int rc = VIE_OK;
+    const long long a = ctx->a;
+    double2* b64 = (double2*)work_vec(ctx, 20, sizeof(double2), &rc);
     if (rc) return rc;
-    rc = finish(ctx, res, 0, 2, PS_RELIABLE, verbose, "mixed BiCGSTAB");
-    updates = ctx->h_ctl->updates;
-    mv64 = updates;
-    return rc;
+    k_mask_rhs<double2><<<kVecBlocks, 256, 0, ctx->stream>>>(ctx->d_rhs, ctx->d_flags, b64, a, 1.0);
+    count_launch();
+    VIE_CUDA_TRY(cudaGetLastError(), ctx->err);
+    DotArgs<double2, 1> g{{b64}, {b64}, {1}};
+    if ((rc = dots(ctx, g))) return rc;
+    if ((rc = finalize<1>(ctx, kVecBlocks, FinNorm{S_BNRM2}))) return rc;
+    if ((rc = read_scalars(ctx))) return rc;
+    *bn2_out = ctx->h_scal[S_BNRM2];
+    *b64_out = b64;
+    if (!(bn2_out->x > 0.0)) return ctx->set_error(VIE_ERR_ARG, "right-hand side is zero on every flagged edge");
+    return VIE_OK;
 }
 
 int solve_driver(vie_ctx* ctx, const vie_solve_params* prm, vie_solve_info* info) {
@@ -1319,21 +1504,10 @@ int solve_driver(vie_ctx* ctx, const vie_solve_params* prm, vie_solve_info* info
     vie_solve_info out{};
     out.steps = -1;
     const long long graphs0 = ctx->graph_launches;
-    // masked right-hand side b (FP64) in work slot 20
-    double2* b64 = (double2*)work_vec(ctx, 20, sizeof(double2), &rc);
-    if (rc) return rc;
-    k_mask_rhs<double2><<<kVecBlocks, 256, 0, st>>>(ctx->d_rhs, ctx->d_flags, b64, a, 1.0);
-    count_launch();
-    VIE_CUDA_TRY(cudaGetLastError(), ctx->err);
-    // ||b||^2
-    {
-        DotArgs<double2, 1> g{{b64}, {b64}, {1}};
-        if ((rc = dots(ctx, g))) return rc;
-        if ((rc = finalize<1>(ctx, kVecBlocks, FinNorm{S_BNRM2}))) return rc;
-        if ((rc = read_scalars(ctx))) return rc;
-    }
-    double2 bn2 = ctx->h_scal[S_BNRM2];
-    if (!(bn2.x > 0.0)) return ctx->set_error(VIE_ERR_ARG, "right-hand side is zero on every flagged edge");
+    // masked right-hand side b (FP64) in work slot 20, ||b||^2
+    double2* b64 = nullptr;
+    double2 bn2;
+    if ((rc = prepare_rhs(ctx, &b64, &bn2))) return rc;
     int status = VIE_OK;
     if (prm->precision == VIE_PREC_FP64) {
         KrylovResult res;
@@ -1441,12 +1615,150 @@ int solve_driver(vie_ctx* ctx, const vie_solve_params* prm, vie_solve_info* info
         out.true_relres = -1.0;
     }
     ctx->have_x = true;
+    out.status = status;
     if (info) *info = out;
     if (status == VIE_ERR_MAXIT)
         return ctx->set_error(VIE_ERR_MAXIT, "iteration cap reached before the tolerance");
     if (status == VIE_ERR_BREAKDOWN)
         return ctx->set_error(VIE_ERR_BREAKDOWN, "Krylov breakdown before the tolerance");
     return VIE_OK;
+}
+
+// Several solves (one per context, all on one GPU) in one graph launch.  Each
+// instance is prepared on its own stream (masked right-hand side, set-up of
+// its driver); then one WHILE loop runs, per pass, every live instance's
+// iteration body as a parallel IF branch, until every instance has converged,
+// broken down or reached its cap.  Supported: FP64 with any driver, mixed
+// precision with BiCGSTAB (reliable updates).
+int solve_batch_driver(vie_ctx* const* ctxs, int n, const vie_solve_params* prm, vie_solve_info* infos) {
+    struct Job {
+        vie_ctx* ctx = nullptr;
+        double2* b64 = nullptr;
+        double2 bn2;
+        KrylovResult res;
+        int updates = 0, mv64 = 0;
+        SolvePlan plan;
+        cudaEvent_t ready = nullptr;
+    };
+    vie_ctx* c0 = ctxs[0];
+    const bool mixed = prm->precision == VIE_PREC_MIXED;
+    if (mixed && prm->solver != VIE_SOLVER_BICGSTAB)
+        return c0->set_error(VIE_ERR_ARG, "batched mixed precision is BiCGSTAB only");
+    if (!mixed && prm->precision != VIE_PREC_FP64) return c0->set_error(VIE_ERR_ARG, "unknown precision mode");
+    std::vector<Job> jobs((size_t)n);
+    cudaStream_t S = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int rc = VIE_OK;
+    auto cleanup = [&]() {
+        for (auto& j : jobs)
+            if (j.ready) cudaEventDestroy(j.ready);
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+        if (S) cudaStreamDestroy(S);
+    };
+    if (cudaStreamCreateWithFlags(&S, cudaStreamNonBlocking) != cudaSuccess || cudaEventCreate(&e0) != cudaSuccess ||
+        cudaEventCreate(&e1) != cudaSuccess) {
+        cleanup();
+        return c0->set_error(VIE_ERR_CUDA, "batch stream / events");
+    }
+    cudaEventRecord(e0, S);
+    // prepare every instance on its own stream (after e0, for the timing)
+    for (int i = 0; i < n && !rc; i++) {
+        Job& j = jobs[i];
+        vie_ctx* ctx = j.ctx = ctxs[i];
+        if ((rc = ensure_scalars(ctx))) break;
+        if (cudaStreamWaitEvent(ctx->stream, e0, 0) != cudaSuccess) { rc = ctx->set_error(VIE_ERR_CUDA, "wait"); break; }
+        if ((rc = prepare_rhs(ctx, &j.b64, &j.bn2))) break;
+        const int maxit = prm->max_iter > 0 ? prm->max_iter : (int)std::min<long long>(ctx->a, 2000000000LL);
+        if (mixed) {
+            const double delta = prm->inner_tol > 0 ? prm->inner_tol : 0.1;
+            rc = solve_bicgstab_mixed(ctx, j.b64, ctx->d_x, prm->tol, delta, maxit, prm->verbose, j.res, j.updates,
+                                      j.mv64, &j.plan);
+        } else {
+            rc = run_solver<double>(ctx, ctx->op64, prm->solver, j.b64, ctx->d_x, prm->tol, maxit, prm->verbose, 0,
+                                    j.res, &j.plan);
+        }
+        if (rc) break;
+        if (cudaEventCreate(&j.ready) != cudaSuccess || cudaEventRecord(j.ready, ctx->stream) != cudaSuccess ||
+            cudaStreamWaitEvent(S, j.ready, 0) != cudaSuccess) {
+            rc = ctx->set_error(VIE_ERR_CUDA, "batch set-up events");
+            break;
+        }
+    }
+    if (rc) {
+        if (c0->err.code == VIE_OK && rc) c0->set_error(rc, "batch set-up failed");
+        cleanup();
+        return rc;
+    }
+    std::vector<SolvePlan*> plans;
+    for (auto& j : jobs) plans.push_back(&j.plan);
+    bool launched = false;
+    if (c0->use_graphs) rc = run_loop_batch_graph(plans, S, c0, launched);
+    if (!launched) {
+        // the graph could not be built (nothing ran) or graphs are off: the
+        // same bodies round-robin from the host, states read back every pass
+        if (rc) std::fprintf(stderr, "vie_b200: %s; batch iterating without graphs\n", c0->err.msg.c_str());
+        rc = VIE_OK;
+        c0->err.code = VIE_OK;
+        cudaStreamSynchronize(S);
+        std::vector<char> live((size_t)n, 1);
+        for (bool any = true; any && !rc;) {
+            any = false;
+            for (int i = 0; i < n && !rc; i++) {
+                if (!live[i]) continue;
+                vie_ctx* c = jobs[i].ctx;
+                if ((rc = plans[i]->body())) break;
+                c->gate = Gate{nullptr, 0};
+                k_loop_count<<<1, 1, 0, c->stream>>>(c->d_ctl);
+                count_launch();
+            }
+            for (int i = 0; i < n && !rc; i++) {
+                if (!live[i]) continue;
+                if ((rc = ctl_read(jobs[i].ctx))) break;
+                live[i] = ks_live(jobs[i].ctx->h_ctl->state);
+                any = any || live[i];
+            }
+        }
+        for (auto& j : jobs) cudaEventRecord(j.ready, j.ctx->stream), cudaStreamWaitEvent(S, j.ready, 0);
+    }
+    if (rc) {
+        cleanup();
+        return rc;
+    }
+    cudaEventRecord(e1, S);
+    cudaEventSynchronize(e1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    int first_err = VIE_OK;
+    for (int i = 0; i < n; i++) {
+        Job& j = jobs[i];
+        vie_ctx* ctx = j.ctx;
+        int frc = j.plan.finish();
+        vie_solve_info out{};
+        out.steps = j.res.steps;
+        out.iterations = j.res.iterations;
+        out.relres = j.res.err;
+        if (mixed) {
+            out.outer = j.updates;
+            out.matvecs_fp32 = j.res.matvecs;
+            out.matvecs_fp64 = j.mv64;
+            out.true_relres = j.res.err;
+        } else {
+            out.matvecs_fp64 = j.res.matvecs;
+            out.true_relres = -1.0;
+        }
+        out.seconds = ms * 1e-3;
+        out.graph_loops = launched ? 1 : 0;
+        ctx->have_x = true;
+        int status = frc;
+        if (!status && j.res.status == VIE_ERR_MAXIT)
+            status = ctx->set_error(VIE_ERR_MAXIT, "iteration cap reached before the tolerance");
+        out.status = status;
+        if (infos) infos[i] = out;
+        if (status && !first_err) first_err = status;
+    }
+    cleanup();
+    return first_err;
 }
 
 // ||b - A x|| / ||b|| of the current solution in FP64 (one operator application)

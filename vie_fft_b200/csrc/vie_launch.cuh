@@ -39,11 +39,9 @@ template <typename T> inline long long epilogue_blocks(const Operator<T>& op) {
     int rows = op.dev.tz;
     if (op.dev.fast[2]) {
         switch (op.dev.nz) {
-            case 256: rows = fast_rows<C, 256>(); break;
-            case 128: rows = fast_rows<C, 128>(); break;
-            case 64: rows = fast_rows<C, 64>(); break;
-            case 32: rows = fast_rows<C, 32>(); break;
-            case 16: rows = fast_rows<C, 16>(); break;
+#define VIE_ROWS_CASE(NN) case NN: rows = fast_rows<C, NN>(); break;
+            VIE_FAST_LENGTHS(VIE_ROWS_CASE)
+#undef VIE_ROWS_CASE
         }
     }
     return (long long)ceil_div(nrows, rows) * 3;
@@ -103,14 +101,22 @@ int launch_fast_x(Operator<T>& op, bool conj, cudaStream_t st, Error& err) {
     return VIE_OK;
 }
 
-#define VIE_FAST_SWITCH(n, CALL)                             \
-    switch (n) {                                              \
-        case 256: { constexpr int NN = 256; CALL; } break;    \
-        case 128: { constexpr int NN = 128; CALL; } break;    \
-        case 64: { constexpr int NN = 64; CALL; } break;      \
-        case 32: { constexpr int NN = 32; CALL; } break;      \
-        case 16: { constexpr int NN = 16; CALL; } break;      \
-        default: break;                                       \
+#define VIE_FAST_SWITCH(n, CALL)                                   \
+    switch (n) {                                                    \
+        case 256: { constexpr int NN = 256; CALL; } break;          \
+        case 128: { constexpr int NN = 128; CALL; } break;          \
+        case 96: { constexpr int NN = 96; CALL; } break;            \
+        case 88: { constexpr int NN = 88; CALL; } break;            \
+        case 80: { constexpr int NN = 80; CALL; } break;            \
+        case 72: { constexpr int NN = 72; CALL; } break;            \
+        case 64: { constexpr int NN = 64; CALL; } break;            \
+        case 56: { constexpr int NN = 56; CALL; } break;            \
+        case 48: { constexpr int NN = 48; CALL; } break;            \
+        case 40: { constexpr int NN = 40; CALL; } break;            \
+        case 32: { constexpr int NN = 32; CALL; } break;            \
+        case 24: { constexpr int NN = 24; CALL; } break;            \
+        case 16: { constexpr int NN = 16; CALL; } break;            \
+        default: break;                                             \
     }
 
 // y = A x (or A^H x) with a prologue producing the source values and an

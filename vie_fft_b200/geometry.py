@@ -277,3 +277,41 @@ def design_stack(shape=(128, 128, 64), voxel_nm=1.0, spacer_nm=16.0, active_top_
     return Workload("design_stack", tuple(shape), (d, d, d), k0_of(wavelength_nm), mat, flags, table,
                     eps_voxel=eps, cross_section=nx * d * ny * d,
                     meta={"region": region, "wavelength_nm": wavelength_nm})
+
+
+def batch_sweep(shape=(96, 96, 48), voxel_nm=1.0, n_wavelengths=64, wavelength_range_nm=(350.0, 800.0),
+                psis=(0.0, 90.0), spacer_nm=8.0, active_nm=24.0, nspheres=4, radius_nm=8.0,
+                sphere_z_nm=(16.0, 24.0), seed=4):
+    """Wavelength x polarisation sweep over one solar-cell grid: the 256^3 stack
+    scaled to a 48-voxel height (spacer 8 nm, active layer 24 nm, Ag spheres of
+    radius 8 nm in the active layer), silver from the Drude model at each
+    wavelength (drude_silver), the layers at their fixed permittivities;
+    polarisation x (psi = 0) and y (psi = 90).  Returns the list of
+    n_wavelengths * len(psis) workloads (all on the same grid)."""
+    base = solar_cell(shape=shape, voxel_nm=voxel_nm, spacer_nm=spacer_nm, active_nm=active_nm, nspheres=nspheres,
+                      radius_nm=radius_nm, sphere_z_nm=sphere_z_nm, seed=seed)
+    out = []
+    for lam in np.linspace(wavelength_range_nm[0], wavelength_range_nm[1], n_wavelengths):
+        table = base.eps_table.copy()
+        table[2] = to_reference_eps(drude_silver(lam))
+        for psi in psis:
+            out.append(Workload("batch_sweep", base.shape, base.d, k0_of(lam), base.material, base.flags, table,
+                                psi=psi, cross_section=base.cross_section,
+                                meta={"wavelength_nm": float(lam), "psi": psi}))
+    return out
+
+
+def batch_spheres(count=48, edges=tuple(range(16, 97, 8)), voxel_nm=1.0, wavelength_nm=550.0, seed=4):
+    """Single spheres on uneven grids: edge n drawn from `edges`, diameter (n - 2)
+    voxels, permittivity Re uniform in [-6, -1], Im uniform in [0.1, 1.0]
+    (physics convention)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        n = int(rng.choice(np.asarray(edges)))
+        eps = rng.uniform(-6.0, -1.0) + 1j * rng.uniform(0.1, 1.0)
+        w = single_sphere(n=n, voxel_nm=voxel_nm, diameter_nm=(n - 2) * voxel_nm, eps_physics=eps,
+                          wavelength_nm=wavelength_nm)
+        w.meta["eps_physics"] = eps
+        out.append(w)
+    return out
