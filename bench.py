@@ -493,6 +493,110 @@ def run_gpu_batch(args, rank, world, local_rank):
         c.close()
 
 
+def run_gpu_gradient(args, rank, world, local_rank):
+    """Adjoint gradient of the active-layer absorption summed over 450, 550 and
+    650 nm (x-polarised) on the 128x128x64 design stack (64x64x32 design
+    region, seed 5).  value = gradient evaluations/s with mixed-precision forward
+    and adjoint solves; also FP64, the agreement of the two, and FP64 central
+    differences (h = 1e-6 on Re and Im) at 32 seeded design voxels (seed 6)."""
+    import numpy as np
+    import torch
+
+    import vie_fft_b200 as V
+    from vie_fft_b200 import geometry as G
+    from vie_fft_b200 import post
+
+    torch.cuda.set_device(local_rank)
+    lams = (450.0, 550.0, 650.0)
+    ws = [G.design_stack(wavelength_nm=lam) for lam in lams]
+    mask = post.edge_mask(ws[0].material, 3)
+    ctxs = []
+    for w in ws:
+        c = V.Context(*w.shape, *w.d, w.k0, device=local_rank)
+        c.set_flags(w.flags)
+        c.set_eps(w.eps_voxel)
+        c.green()
+        c.incident(w.theta, w.phi, w.psi, copy=False)
+        ctxs.append(c)
+
+    def evaluate(precision, tol, grad=True):
+        p, g, its = 0.0, 0.0, []
+        for c in ctxs:
+            pi, gi, fi, ai = c.power_grad(mask, tol=tol, precision=precision, grad=grad)
+            p += pi
+            if grad:
+                g = g + gi
+            its.append((fi["iterations"], ai["iterations"]))
+        return p, g, its
+
+    for _ in range(args.warmup):
+        evaluate(V.PREC_MIXED, TOL)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local_rank) if rank == 0 else None
+    launches0 = V.launch_count()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        pm, gm, itm = evaluate(V.PREC_MIXED, TOL)
+    torch.cuda.synchronize()
+    t_mixed = (time.perf_counter() - t0) / args.steps
+    launches = (V.launch_count() - launches0) // args.steps
+    clocks = sampler.stop() if sampler else None
+    t0 = time.perf_counter()
+    p64, g64, it64 = evaluate(V.PREC_FP64, TOL)
+    torch.cuda.synchronize()
+    t64 = time.perf_counter() - t0
+    # central differences of the FP64 objective at 32 design voxels
+    region = np.argwhere(ws[0].meta["region"])
+    rng = np.random.default_rng(6)
+    picks = [tuple(region[i]) for i in rng.choice(len(region), 32, replace=False)]
+    # the FP64 solves of the differences go to 1e-13 (capped at 5000 iterations):
+    # with h = 1e-6 the difference quotient carries the solve error / h
+    h, fd_tol = 1e-6, 1e-13
+    _, gref, _ = evaluate(V.PREC_FP64, fd_tol)
+    scale = float(np.abs(gref[ws[0].meta["region"]]).max())
+    errs = []
+    for v in picks:
+        fd = []
+        for dz in (h, 1j * h):
+            vals = []
+            for sgn in (1.0, -1.0):
+                tot = 0.0
+                for w, c in zip(ws, ctxs):
+                    eps = w.eps_voxel.copy()
+                    eps[v] += sgn * dz
+                    c.set_eps(eps)
+                    tot += c.power_grad(mask, tol=fd_tol, grad=False, max_iter=5000)[0]
+                vals.append(tot)
+            fd.append((vals[0] - vals[1]) / (2 * h))
+        errs.append(abs(gref[v] - (fd[0] + 1j * fd[1])) / scale)
+    worst = max(errs)
+    for w, c in zip(ws, ctxs):
+        c.set_eps(w.eps_voxel)
+    line = {
+        "metric": "adjoint gradient evaluations/s (absorbed power in the active layer, 3 wavelengths, "
+                  "forward + adjoint solves to rel-res 1e-8)",
+        "value": 1.0 / t_mixed, "unit": "gradients/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t_mixed * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "c64 inner + c128 refine", "data": "synthetic",
+        "config": {"workload": "128x128x64 solar-cell stack, 64x64x32 design region (eps Re[1,4] Im[0,0.5], "
+                               "seed 5), 450/550/650 nm x-pol, objective = NearField Ene_Active sum",
+                   "design_voxels": int(ws[0].meta["region"].sum())},
+        "fp64": {"gradients_per_s": 1.0 / t64, "iterations_fwd_adj": it64},
+        "mixed": {"iterations_fwd_adj": itm},
+        "speedup_mixed_vs_fp64": t64 / t_mixed,
+        "power": {"mixed": pm, "fp64": p64, "rel_diff": abs(pm - p64) / abs(p64)},
+        "grad_rel_diff_mixed_vs_fp64": float(np.abs(gm - g64).max() / np.abs(g64).max()),
+        "fd_check": {"voxels": 32, "h": h, "solve_tol": fd_tol,
+                     "max_abs_err_over_max_grad": worst, "median_abs_err_over_max_grad": float(np.median(errs)),
+                     "max_grad": scale},
+        "gpu_launches": launches, "clocks": clocks,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    for c in ctxs:
+        c.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -500,7 +604,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="vie", choices=["vie", "reference"])
     ap.add_argument("--workload", default="c3",
-                    help="c1 | c2 | c3 | c4 (batched: c4i sweep, c4ii spheres), or grid:NX,NY,NZ "
+                    help="c1 | c2 | c3 | c4 (batched: c4i sweep, c4ii spheres) | c5 (adjoint gradient), "
+                         "or grid:NX,NY,NZ "
                          "(synthetic operator, --only-matvec)")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
@@ -526,6 +631,8 @@ def main():
     try:
         if args.workload.startswith("c4"):
             run_gpu_batch(args, rank, world, local_rank)
+        elif args.workload == "c5":
+            run_gpu_gradient(args, rank, world, local_rank)
         else:
             run_gpu(args, rank, world, local_rank)
     finally:

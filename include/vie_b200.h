@@ -175,6 +175,20 @@ VIE_API int vie_solve(vie_ctx* ctx, const vie_solve_params* p, double* x, vie_so
    instance's counts, `seconds` being the time of the whole batch.  Returns
    the first non-OK instance status (VIE_ERR_MAXIT if any instance hit its cap). */
 VIE_API int vie_solve_batch(vie_ctx* const* ctxs, int n, const vie_solve_params* p, vie_solve_info* infos);
+/* Absorbed power in a set of edges and its gradient with respect to the
+   per-voxel complex permittivity (no reference counterpart; the objective is
+   the absorption sum of NearField, NearFar.h:186-250, restricted to the
+   edges whose bit is set in edge_mask: bit f of byte v selects the f-edge of
+   voxel v, e.g. Ene_Active = edges whose two voxels are both active, with
+   i, j, k < N - 1).  Runs the forward solve with p (J), *power = P, and, if
+   grad != NULL, one adjoint solve with the same driver and precision on the
+   conjugated source (the operator is complex-symmetric for cubic voxels,
+   which this requires) and grad[v] = dP/dRe(eps_v) + i dP/dIm(eps_v) for the
+   permittivity in the convention of vie_set_eps (a complex).  The context
+   keeps its right-hand side; its solution is the forward field afterwards.
+   info_fwd / info_adj (may be NULL) receive the two solves' counts. */
+VIE_API int vie_power_grad(vie_ctx* ctx, const unsigned char* edge_mask, const vie_solve_params* p, double* power,
+                           double* grad, vie_solve_info* info_fwd, vie_solve_info* info_adj);
 /* ||b - A x|| / ||b|| of the last solution for the current right-hand side,
    evaluated in FP64 (one operator application). */
 VIE_API int vie_residual(vie_ctx* ctx, double* relres);

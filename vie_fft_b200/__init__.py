@@ -103,6 +103,7 @@ def lib():
         L.vie_matvec_dev.argtypes = [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int]
         L.vie_solve.argtypes = [_vp, P(VieSolveParams), _dp, P(VieSolveInfo)]
         L.vie_solve_batch.argtypes = [P(_vp), ctypes.c_int, P(VieSolveParams), P(VieSolveInfo)]
+        L.vie_power_grad.argtypes = [_vp, _up, P(VieSolveParams), _dp, _dp, P(VieSolveInfo), P(VieSolveInfo)]
         L.vie_get_solution.argtypes = [_vp, _dp]
         L.vie_residual.argtypes = [_vp, _dp]
         L.vie_solution_device.argtypes = [_vp, P(_vp)]
@@ -242,6 +243,25 @@ class Context:
         rc = self._L.vie_solve(self._h, ctypes.byref(prm), _p(x) if copy else None, ctypes.byref(info))
         self._check(rc, allow=(VIE_ERR_MAXIT,) if allow_maxit else ())
         return SolveResult(x, info.as_dict(), rc)
+
+    def power_grad(self, edge_mask, solver="bicgstab", tol=1e-8, precision=PREC_FP64, grad=True, max_iter=0,
+                   inner_tol=0.0):
+        """Absorbed power P in the edges of ``edge_mask`` (uint8 per voxel, bit f =
+        the f-edge; see post.edge_mask) and, with ``grad``, dP/dRe(eps) + i dP/dIm(eps)
+        per voxel for the permittivity as given to set_eps / set_material
+        (``vie_power_grad``: forward solve + one adjoint solve).
+        Returns (P, grad (nx, ny, nz) complex or None, forward info, adjoint info)."""
+        m = np.ascontiguousarray(edge_mask, np.uint8)
+        if m.shape != self.shape:
+            raise ValueError(f"edge_mask must have shape {self.shape}")
+        prm = VieSolveParams(SOLVERS[solver] if isinstance(solver, str) else int(solver), int(precision), float(tol),
+                             int(max_iter), float(inner_tol), 0, 0, 0)
+        pw = ctypes.c_double(0.0)
+        g = np.zeros(self.shape, np.complex128) if grad else None
+        fi, ai = VieSolveInfo(), VieSolveInfo()
+        self._check(self._L.vie_power_grad(self._h, _p(m, _up), ctypes.byref(prm), ctypes.byref(pw),
+                                           _p(g) if grad else None, ctypes.byref(fi), ctypes.byref(ai)))
+        return pw.value, g, fi.as_dict(), ai.as_dict()
 
     def residual(self) -> float:
         """||b - A x|| / ||b|| of the last solution, in FP64."""

@@ -14,6 +14,8 @@ int green_expand(vie_ctx* ctx, double2* d_out);
 int incident_compute(vie_ctx* ctx, double theta, double phi, double psi, double2* d_e);
 int solve_driver(vie_ctx* ctx, const vie_solve_params* prm, vie_solve_info* info);
 int solve_batch_driver(vie_ctx* const* ctxs, int n, const vie_solve_params* prm, vie_solve_info* infos);
+int power_grad_driver(vie_ctx* ctx, const unsigned char* edge_mask, const vie_solve_params* prm, double* power,
+                      double* grad, vie_solve_info* info_fwd, vie_solve_info* info_adj);
 int residual_driver(vie_ctx* ctx, double* relres);
 void mask_component(double2* v, const unsigned char* flags, long long a, int comp, cudaStream_t st);
 }  // namespace vie
@@ -358,6 +360,23 @@ int vie_solve_batch(vie_ctx* const* ctxs, int n, const vie_solve_params* p, vie_
     if (!(p->tol > 0)) return ctxs[0]->set_error(VIE_ERR_ARG, "tolerance must be positive");
     cudaSetDevice(ctxs[0]->device);
     return solve_batch_driver(ctxs, n, p, infos);
+}
+
+int vie_power_grad(vie_ctx* ctx, const unsigned char* edge_mask, const vie_solve_params* p, double* power,
+                   double* grad, vie_solve_info* info_fwd, vie_solve_info* info_adj) {
+    if (check_ctx(ctx) || !edge_mask || !p || !power) return VIE_ERR_ARG;
+    int rc = ready_for_operator(ctx);
+    if (rc) return rc;
+    if (!ctx->have_rhs) return ctx->set_error(VIE_ERR_STATE, "no right-hand side (vie_incident / vie_set_rhs)");
+    if (!(p->tol > 0)) return ctx->set_error(VIE_ERR_ARG, "tolerance must be positive");
+    if (grad && !(ctx->d[0] == ctx->d[1] && ctx->d[1] == ctx->d[2]))
+        return ctx->set_error(VIE_ERR_ARG, "the adjoint gradient needs cubic voxels (complex-symmetric operator)");
+    cudaSetDevice(ctx->device);
+    ctx->err.code = VIE_OK;
+    ctx->err.msg.clear();
+    rc = power_grad_driver(ctx, edge_mask, p, power, grad, info_fwd, info_adj);
+    if (!rc) ctx->have_x = true;
+    return rc;
 }
 
 int vie_residual(vie_ctx* ctx, double* relres) {

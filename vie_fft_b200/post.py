@@ -57,6 +57,22 @@ def absorption(shape, d, k0, x, eps, material, metal_label=2, active_label=3):
     return em, ea, av
 
 
+def edge_mask(material, label=3):
+    """Edge set of NearField's per-material sum (NearFar.h:186-250): bit f of voxel
+    (i, j, k) is set when i, j, k < N - 1 and the voxel and its +f neighbour both
+    hold ``label`` (3: Ene_Active, 2: Ene_Metal)."""
+    m = np.asarray(material)
+    nx, ny, nz = m.shape
+    out = np.zeros(m.shape, np.uint8)
+    core = (slice(0, nx - 1), slice(0, ny - 1), slice(0, nz - 1))
+    for f in range(3):
+        nb = [slice(0, nx - 1), slice(0, ny - 1), slice(0, nz - 1)]
+        nb[f] = slice(1, m.shape[f])
+        sel = (m[core] == label) & (m[tuple(nb)] == label)
+        out[core] |= (sel.astype(np.uint8) << f)
+    return out
+
+
 def cross_sections(w, x) -> dict:
     """Extinction and absorption efficiencies of a Workload's solution."""
     fwd = forward_scattering(w.shape, w.d, w.k0, x, w.theta, w.phi, w.psi)
