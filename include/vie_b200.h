@@ -189,6 +189,19 @@ VIE_API int vie_solve_batch(vie_ctx* const* ctxs, int n, const vie_solve_params*
    info_fwd / info_adj (may be NULL) receive the two solves' counts. */
 VIE_API int vie_power_grad(vie_ctx* ctx, const unsigned char* edge_mask, const vie_solve_params* p, double* power,
                            double* grad, vie_solve_info* info_fwd, vie_solve_info* info_adj);
+/* Autotuner of the FFT schedule (no reference counterpart).  Times, for this
+   context's grid, the candidate schedules of each axis (register four-step
+   kernels where the length has them; generic shared-memory kernels with the
+   default, reversed and 16 -> 4x4 / 8x2 radix orders and pencil tiles around
+   the default) and rebuilds the operators with the fastest.  flags: 1 FP64,
+   2 FP32 (0: both), 4 tune again even when the process already has a choice
+   for this grid.  Choices are shared by every later context with the same
+   grid and device in the process, and kept in the text file named by the
+   environment variable VIE_TUNE_CACHE when set; VIE_AUTOTUNE=1 tunes each new
+   grid automatically.  report (may be NULL) receives a one-line summary.
+   Needs vie_set_flags first; results do not depend on the schedule beyond
+   rounding. */
+VIE_API int vie_autotune(vie_ctx* ctx, int flags, char* report, int report_len);
 /* ||b - A x|| / ||b|| of the last solution for the current right-hand side,
    evaluated in FP64 (one operator application). */
 VIE_API int vie_residual(vie_ctx* ctx, double* relres);

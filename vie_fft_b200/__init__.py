@@ -103,6 +103,7 @@ def lib():
         L.vie_matvec_dev.argtypes = [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int]
         L.vie_solve.argtypes = [_vp, P(VieSolveParams), _dp, P(VieSolveInfo)]
         L.vie_solve_batch.argtypes = [P(_vp), ctypes.c_int, P(VieSolveParams), P(VieSolveInfo)]
+        L.vie_autotune.argtypes = [_vp, ctypes.c_int, ctypes.c_char_p, ctypes.c_int]
         L.vie_power_grad.argtypes = [_vp, _up, P(VieSolveParams), _dp, _dp, P(VieSolveInfo), P(VieSolveInfo)]
         L.vie_get_solution.argtypes = [_vp, _dp]
         L.vie_residual.argtypes = [_vp, _dp]
@@ -262,6 +263,14 @@ class Context:
         self._check(self._L.vie_power_grad(self._h, _p(m, _up), ctypes.byref(prm), ctypes.byref(pw),
                                            _p(g) if grad else None, ctypes.byref(fi), ctypes.byref(ai)))
         return pw.value, g, fi.as_dict(), ai.as_dict()
+
+    def autotune(self, fp64=True, fp32=True, force=False) -> str:
+        """Time the FFT schedules of this grid and rebuild the operators with the
+        fastest (``vie_autotune``); returns the one-line report."""
+        flags = (1 if fp64 else 0) | (2 if fp32 else 0) | (4 if force else 0)
+        buf = ctypes.create_string_buffer(1024)
+        self._check(self._L.vie_autotune(self._h, flags, buf, len(buf)))
+        return buf.value.decode()
 
     def residual(self) -> float:
         """||b - A x|| / ||b|| of the last solution, in FP64."""

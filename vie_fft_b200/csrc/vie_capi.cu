@@ -14,6 +14,8 @@ int green_expand(vie_ctx* ctx, double2* d_out);
 int incident_compute(vie_ctx* ctx, double theta, double phi, double psi, double2* d_e);
 int solve_driver(vie_ctx* ctx, const vie_solve_params* prm, vie_solve_info* info);
 int solve_batch_driver(vie_ctx* const* ctxs, int n, const vie_solve_params* prm, vie_solve_info* infos);
+void tune_apply_cached(vie_ctx* ctx);
+int autotune_driver(vie_ctx* ctx, int flags);
 int power_grad_driver(vie_ctx* ctx, const unsigned char* edge_mask, const vie_solve_params* prm, double* power,
                       double* grad, vie_solve_info* info_fwd, vie_solve_info* info_adj);
 int residual_driver(vie_ctx* ctx, double* relres);
@@ -48,10 +50,23 @@ TileCfg tiles_from_env() {
 
 int ensure_operators(vie_ctx* ctx) {
     if (ctx->op64.ready && ctx->op32.ready) return VIE_OK;
-    TileCfg t = tiles_from_env();
-    int rc = ctx->op64.init(ctx->nx, ctx->ny, ctx->nz, ctx->d, ctx->k0, t, ctx->plans, ctx->d_flags, ctx->err);
+    if (!ctx->sched_set) {
+        // defaults (VIE_TILES), replaced by a tuned schedule of this grid when
+        // the process has one (vie_autotune, VIE_TUNE_CACHE); VIE_AUTOTUNE=1
+        // tunes every new grid shape on first use
+        ctx->sched64 = ctx->sched32 = tiles_from_env();
+        for (int ax = 0; ax < 3; ax++) ctx->plans64[ax] = ctx->plans32[ax] = ctx->plans[ax];
+        ctx->sched_set = true;
+        tune_apply_cached(ctx);
+    }
+    int rc = ctx->op64.init(ctx->nx, ctx->ny, ctx->nz, ctx->d, ctx->k0, ctx->sched64, ctx->plans64, ctx->d_flags,
+                            ctx->err);
     if (rc) return rc;
-    rc = ctx->op32.init(ctx->nx, ctx->ny, ctx->nz, ctx->d, ctx->k0, t, ctx->plans, ctx->d_flags, ctx->err);
+    rc = ctx->op32.init(ctx->nx, ctx->ny, ctx->nz, ctx->d, ctx->k0, ctx->sched32, ctx->plans32, ctx->d_flags,
+                        ctx->err);
+    if (rc) return rc;
+    if (const char* at = std::getenv("VIE_AUTOTUNE"))
+        if (at[0] == '1' && ctx->tune_report.empty()) rc = autotune_driver(ctx, 0);
     return rc;
 }
 
@@ -376,6 +391,18 @@ int vie_power_grad(vie_ctx* ctx, const unsigned char* edge_mask, const vie_solve
     ctx->err.msg.clear();
     rc = power_grad_driver(ctx, edge_mask, p, power, grad, info_fwd, info_adj);
     if (!rc) ctx->have_x = true;
+    return rc;
+}
+
+int vie_autotune(vie_ctx* ctx, int flags, char* report, int report_len) {
+    if (check_ctx(ctx)) return VIE_ERR_ARG;
+    if (!ctx->have_flags) return ctx->set_error(VIE_ERR_STATE, "edge flags not set (vie_set_flags)");
+    cudaSetDevice(ctx->device);
+    int rc = ensure_operators(ctx);
+    if (!rc) rc = autotune_driver(ctx, flags);
+    if (report && report_len > 0) {
+        std::snprintf(report, (size_t)report_len, "%s", ctx->tune_report.c_str());
+    }
     return rc;
 }
 

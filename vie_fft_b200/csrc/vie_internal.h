@@ -45,6 +45,7 @@ std::vector<int> axis_perm(const AxisPlan& pl);
 // Tile sizes of the five passes for one precision.
 struct TileCfg {
     int tz = 0, tc = 0, tx = 0;
+    int fast[3] = {-1, -1, -1};  // per axis: 1 register four-step kernels, 0 generic, -1 automatic
 };
 
 // Operator state for one arithmetic precision.  Owns its tables, the Green
@@ -123,6 +124,11 @@ struct vie_ctx {
     double2* d_green = nullptr;           // (nx+1)(ny+1)(nz+1)
     bool have_green = false;
     vie::AxisPlan plans[3];
+    // FFT schedule of each precision (autotuner choice or defaults)
+    vie::TileCfg sched64, sched32;
+    vie::AxisPlan plans64[3], plans32[3];
+    bool sched_set = false;
+    std::string tune_report;
     vie::Operator<double> op64;
     vie::Operator<float> op32;
 
