@@ -370,6 +370,14 @@ def run_gpu(args, rank, world, local_rank):
     cs_64 = post.cross_sections(w, x64)
     xerr = {k: abs(cs_mixed[k] - cs_64[k]) / max(abs(cs_64[k]), 1e-300) for k in cs_64}
     field_rel = float(np.linalg.norm(x_mixed - x64) / np.linalg.norm(x64))
+    # ---- post-processing of the solution on the GPU (FarField1, FarField2, NearField)
+    post_ms = {}
+    for name, fn in (("farfield1", lambda: c.farfield1(w.theta, w.phi, w.psi)), ("farfield2", lambda: c.farfield2(w.phi)),
+                     ("nearfield", lambda: c.nearfield(w.material))):
+        fn()
+        t0 = time.perf_counter()
+        fn()
+        post_ms[name] = (time.perf_counter() - t0) * 1e3
 
     # ---- CPU baseline (bounded sample), rank 0 at N = 1 only
     cpu = None
@@ -409,6 +417,7 @@ def run_gpu(args, rank, world, local_rank):
         "matvec_hbm_frac": {"fp32": ach32 / peak, "fp64": ach64 / peak},
         "xsec_rel_err_mixed_vs_fp64": xerr, "field_rel_diff_mixed_vs_fp64": field_rel,
         "green_setup_s": green_s, "fft_schedule": schedule, "autotune_s": tune_s,
+        "post_ms_gpu": post_ms,
     }
     print(json.dumps(line), flush=True)
     c.close()

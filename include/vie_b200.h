@@ -189,6 +189,18 @@ VIE_API int vie_solve_batch(vie_ctx* const* ctxs, int n, const vie_solve_params*
    info_fwd / info_adj (may be NULL) receive the two solves' counts. */
 VIE_API int vie_power_grad(vie_ctx* ctx, const unsigned char* edge_mask, const vie_solve_params* p, double* power,
                            double* grad, vie_solve_info* info_fwd, vie_solve_info* info_adj);
+/* Post-processing of the last solution on the GPU (the field stays on the
+   device).  vie_farfield1 replaces FarField1 (NearFar.h:16-109): Forward_RCS
+   for the incidence angles theta, phi, psi (degrees).  vie_farfield2 replaces
+   FarField2 (NearFar.h:302-477): the 181 E-plane (phi) and 181 H-plane
+   (phi + 90) RCS values in dB, theta = 0..180.  vie_nearfield replaces the
+   absorption sums of NearField (NearFar.h:186-250): Ene_Metal, Ene_Active and
+   Absorb_Volume from the material labels (2 metal, 3 active; a bytes). */
+VIE_API int vie_farfield1(vie_ctx* ctx, double theta, double phi, double psi, double* forward_rcs);
+VIE_API int vie_farfield2(vie_ctx* ctx, double phi, double* rcs_theta, double* rcs_phi);
+VIE_API int vie_nearfield(vie_ctx* ctx, const uint8_t* material, double* ene_metal, double* ene_active,
+                          double* absorb_volume);
+
 /* Autotuner of the FFT schedule (no reference counterpart).  Times, for this
    context's grid, the candidate schedules of each axis (register four-step
    kernels where the length has them; generic shared-memory kernels with the
@@ -207,6 +219,9 @@ VIE_API int vie_autotune(vie_ctx* ctx, int flags, char* report, int report_len);
 VIE_API int vie_residual(vie_ctx* ctx, double* relres);
 /* Copy the last solution (Current_X/Y/Z) to the host, 3a complex. */
 VIE_API int vie_get_solution(vie_ctx* ctx, double* x);
+/* Replace the solution by a given current (3a complex, the layout of
+   Current_X/Y/Z), e.g. to post-process a field computed elsewhere. */
+VIE_API int vie_set_solution(vie_ctx* ctx, const double* x);
 /* Device pointer of the last solution (3a double2), valid until the next solve. */
 VIE_API int vie_solution_device(vie_ctx* ctx, const void** x);
 

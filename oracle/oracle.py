@@ -277,6 +277,11 @@ class Reference:
         self.L.ref_farfield1(ctypes.byref(v))
         return v.value
 
+    def farfield2(self):
+        rt, rp = np.zeros(181), np.zeros(181)
+        self.L.ref_farfield2(_p(rt), _p(rp))
+        return rt, rp
+
     def nearfield(self):
         e = ctypes.c_double(0)
         m = ctypes.c_double(0)

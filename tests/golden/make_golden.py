@@ -15,6 +15,8 @@ Fixtures
   c1_sphere.npz      the 32^3 silver-sphere BiCGSTAB solve to 1e-6: step
                      count, solution on the flagged edges, FarField1 and
                      NearField outputs
+  post_ops.npz       FarField1, FarField2 (RCS) and NearField outputs of the
+                     reference on seeded currents of the small cases
   dropin_blocks.npz  X/Y/Z_FFT rows, L_DC_Dq, L_Dq, L??_DO (and conjugate
                      twins) and Current_Reset on small seeded cases
   dropin_program.npz the reference's unchanged main program (CG_FFT_VIE.cpp,
@@ -115,6 +117,23 @@ def make_c1():
                         forward_rcs=fwd, ext_over_cs=ext, metal_abs_over_cs=metal)
 
 
+def make_post_ops():
+    out = {}
+    for idx in range(len(SMALL)):
+        shape, d, k0, ang, mat, flags, x = small_inputs(idx)
+        g = O.Grid(*shape, *d, k0)
+        R = O.Reference(g, EPS_TABLE, *ang)
+        R.set_geometry(mat, flags)
+        R.set_cross_section(0.37)
+        R.set_current(x)
+        out[f"ff1_{idx}"] = R.farfield1()
+        rt, rp = R.farfield2()
+        out[f"rcs_theta{idx}"], out[f"rcs_phi{idx}"] = rt, rp
+        out[f"near{idx}"] = np.array(R.nearfield())
+        R.release()
+    np.savez_compressed(os.path.join(OUT, "post_ops.npz"), **out)
+
+
 def make_dropin_blocks():
     out = {}
     for idx in (0, 1, 3):
@@ -189,13 +208,15 @@ def make_dropin_program():
 
 if __name__ == "__main__":
     import sys as _sys
-    which = _sys.argv[1:] or ["ops", "solves", "c1", "blocks", "program"]
+    which = _sys.argv[1:] or ["ops", "solves", "c1", "post", "blocks", "program"]
     if "ops" in which:
         make_small_ops()
     if "solves" in which:
         make_small_solves()
     if "c1" in which:
         make_c1()
+    if "post" in which:
+        make_post_ops()
     if "blocks" in which:
         make_dropin_blocks()
     if "program" in which:

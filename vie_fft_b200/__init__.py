@@ -103,9 +103,13 @@ def lib():
         L.vie_matvec_dev.argtypes = [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int]
         L.vie_solve.argtypes = [_vp, P(VieSolveParams), _dp, P(VieSolveInfo)]
         L.vie_solve_batch.argtypes = [P(_vp), ctypes.c_int, P(VieSolveParams), P(VieSolveInfo)]
+        L.vie_farfield1.argtypes = [_vp] + [ctypes.c_double] * 3 + [_dp]
+        L.vie_farfield2.argtypes = [_vp, ctypes.c_double, _dp, _dp]
+        L.vie_nearfield.argtypes = [_vp, _up, _dp, _dp, _dp]
         L.vie_autotune.argtypes = [_vp, ctypes.c_int, ctypes.c_char_p, ctypes.c_int]
         L.vie_power_grad.argtypes = [_vp, _up, P(VieSolveParams), _dp, _dp, P(VieSolveInfo), P(VieSolveInfo)]
         L.vie_get_solution.argtypes = [_vp, _dp]
+        L.vie_set_solution.argtypes = [_vp, _dp]
         L.vie_residual.argtypes = [_vp, _dp]
         L.vie_solution_device.argtypes = [_vp, P(_vp)]
         L.vie_rhs_device.argtypes = [_vp, P(_vp)]
@@ -264,6 +268,28 @@ class Context:
                                            _p(g) if grad else None, ctypes.byref(fi), ctypes.byref(ai)))
         return pw.value, g, fi.as_dict(), ai.as_dict()
 
+    # -- post-processing of the last solution on the GPU ------------------
+    def farfield1(self, theta=0.0, phi=0.0, psi=0.0) -> float:
+        """Forward_RCS of FarField1 (NearFar.h:16-109)."""
+        v = ctypes.c_double(0)
+        self._check(self._L.vie_farfield1(self._h, float(theta), float(phi), float(psi), ctypes.byref(v)))
+        return v.value
+
+    def farfield2(self, phi=0.0):
+        """(RCS_Theta[181], RCS_Phi[181]) in dB of FarField2 (NearFar.h:302-477)."""
+        rt, rp = np.zeros(181), np.zeros(181)
+        self._check(self._L.vie_farfield2(self._h, float(phi), _p(rt), _p(rp)))
+        return rt, rp
+
+    def nearfield(self, material):
+        """(Ene_Metal, Ene_Active, Absorb_Volume) of NearField (NearFar.h:186-250)."""
+        m = np.ascontiguousarray(material, np.uint8)
+        if m.shape != self.shape:
+            raise ValueError(f"material must have shape {self.shape}")
+        out = [ctypes.c_double(0) for _ in range(3)]
+        self._check(self._L.vie_nearfield(self._h, _p(m, _up), *[ctypes.byref(o) for o in out]))
+        return tuple(o.value for o in out)
+
     def autotune(self, fp64=True, fp32=True, force=False) -> str:
         """Time the FFT schedules of this grid and rebuild the operators with the
         fastest (``vie_autotune``); returns the one-line report."""
@@ -282,6 +308,11 @@ class Context:
         x = np.zeros((3,) + self.shape, np.complex128)
         self._check(self._L.vie_get_solution(self._h, _p(x)))
         return x
+
+    def set_solution(self, x):
+        """Make x (3, nx, ny, nz) the context's solution (for post-processing)."""
+        xx = _c128(x, (3,) + self.shape)
+        self._check(self._L.vie_set_solution(self._h, _p(xx)))
 
     def solution_ptr(self) -> int:
         p = _vp()

@@ -15,6 +15,9 @@ int incident_compute(vie_ctx* ctx, double theta, double phi, double psi, double2
 int solve_driver(vie_ctx* ctx, const vie_solve_params* prm, vie_solve_info* info);
 int solve_batch_driver(vie_ctx* const* ctxs, int n, const vie_solve_params* prm, vie_solve_info* infos);
 void tune_apply_cached(vie_ctx* ctx);
+int farfield1_driver(vie_ctx* ctx, double theta, double phi, double psi, double* fwd);
+int farfield2_driver(vie_ctx* ctx, double phi, double* rcs_theta, double* rcs_phi);
+int nearfield_driver(vie_ctx* ctx, const unsigned char* material, double* out3);
 int autotune_driver(vie_ctx* ctx, int flags);
 int power_grad_driver(vie_ctx* ctx, const unsigned char* edge_mask, const vie_solve_params* prm, double* power,
                       double* grad, vie_solve_info* info_fwd, vie_solve_info* info_adj);
@@ -394,6 +397,42 @@ int vie_power_grad(vie_ctx* ctx, const unsigned char* edge_mask, const vie_solve
     return rc;
 }
 
+static int ready_for_post(vie_ctx* ctx) {
+    if (check_ctx(ctx)) return VIE_ERR_ARG;
+    if (!ctx->have_x) return ctx->set_error(VIE_ERR_STATE, "no solution yet (vie_solve)");
+    cudaSetDevice(ctx->device);
+    return VIE_OK;
+}
+
+int vie_farfield1(vie_ctx* ctx, double theta, double phi, double psi, double* forward_rcs) {
+    int rc = ready_for_post(ctx);
+    if (rc) return rc;
+    if (!forward_rcs) return ctx->set_error(VIE_ERR_ARG, "null output");
+    return farfield1_driver(ctx, theta, phi, psi, forward_rcs);
+}
+
+int vie_farfield2(vie_ctx* ctx, double phi, double* rcs_theta, double* rcs_phi) {
+    int rc = ready_for_post(ctx);
+    if (rc) return rc;
+    if (!rcs_theta || !rcs_phi) return ctx->set_error(VIE_ERR_ARG, "null output");
+    return farfield2_driver(ctx, phi, rcs_theta, rcs_phi);
+}
+
+int vie_nearfield(vie_ctx* ctx, const uint8_t* material, double* ene_metal, double* ene_active,
+                  double* absorb_volume) {
+    int rc = ready_for_post(ctx);
+    if (rc) return rc;
+    if (!material) return ctx->set_error(VIE_ERR_ARG, "null material");
+    if (!ctx->have_eps || !ctx->op64.ready) return ctx->set_error(VIE_ERR_STATE, "permittivity not set");
+    double o[3];
+    rc = nearfield_driver(ctx, material, o);
+    if (rc) return rc;
+    if (ene_metal) *ene_metal = o[0];
+    if (ene_active) *ene_active = o[1];
+    if (absorb_volume) *absorb_volume = o[2];
+    return VIE_OK;
+}
+
 int vie_autotune(vie_ctx* ctx, int flags, char* report, int report_len) {
     if (check_ctx(ctx)) return VIE_ERR_ARG;
     if (!ctx->have_flags) return ctx->set_error(VIE_ERR_STATE, "edge flags not set (vie_set_flags)");
@@ -421,6 +460,15 @@ int vie_get_solution(vie_ctx* ctx, double* x) {
     cudaSetDevice(ctx->device);
     CTX_CUDA(cudaMemcpyAsync(x, ctx->d_x, sizeof(double2) * 3 * (size_t)ctx->a, cudaMemcpyDeviceToHost, ctx->stream));
     CTX_CUDA(cudaStreamSynchronize(ctx->stream));
+    return VIE_OK;
+}
+
+int vie_set_solution(vie_ctx* ctx, const double* x) {
+    if (check_ctx(ctx) || !x) return VIE_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    CTX_CUDA(cudaMemcpyAsync(ctx->d_x, x, sizeof(double2) * 3 * (size_t)ctx->a, cudaMemcpyHostToDevice, ctx->stream));
+    CTX_CUDA(cudaStreamSynchronize(ctx->stream));
+    ctx->have_x = true;
     return VIE_OK;
 }
 
