@@ -77,24 +77,34 @@ template <typename C, int N> __host__ __device__ constexpr size_t fast_smem_row(
     constexpr int A = R1 * (R2 + 1) > R2 * (R1 + 1) ? R1 * (R2 + 1) : R2 * (R1 + 1);
     return sizeof(C) * (2 * (size_t)N + 2 * (size_t)A * fast_rows<C, N>());
 }
-// x pass: E[3][2][R1][R2*TP + TP] (each k1 block padded by TP entries)
-template <typename C, int N> __host__ __device__ constexpr int fast_x_kstride() {
-    return FastPlan<N>::R2 * FastTiles<C>::TP_X + FastTiles<C>::TP_X;
+// x pass: E[3][2][R1][R2*TP + TP] (each k1 block padded by TP entries).  The
+// pencil tile TP of the x pass has two instantiations per precision (the
+// default TP_X and TP_X / 2, chosen per grid by the autotuner).
+template <typename C> __host__ __device__ constexpr int fast_x_tile(int alt) {
+    return alt ? FastTiles<C>::TP_X / 2 : FastTiles<C>::TP_X;
+}
+template <typename C, int N, int TP = FastTiles<C>::TP_X> __host__ __device__ constexpr int fast_x_kstride() {
+    return FastPlan<N>::R2 * TP + TP;
 }
 template <typename C, int N> __host__ __device__ constexpr size_t fast_smem_col() {
     return sizeof(C) * (2 * (size_t)N + 2 * (size_t)N * FastTiles<C>::TP_Y);
 }
-template <typename C, int N> __host__ __device__ constexpr size_t fast_smem_x() {
-    return sizeof(C) * (2 * (size_t)N + 6 * (size_t)FastPlan<N>::R1 * fast_x_kstride<C, N>());
+template <typename C, int N, int TP = FastTiles<C>::TP_X> __host__ __device__ constexpr size_t fast_smem_x() {
+    return sizeof(C) * (2 * (size_t)N + 6 * (size_t)FastPlan<N>::R1 * fast_x_kstride<C, N, TP>());
 }
 
 // launch bounds: threads per CTA and the CTAs per SM the register allocation must allow
 template <typename C, int N> struct FastLB;
+// (x pass: 3 * 16 * TP threads, and as many CTAs per SM as keep the register
+// cap of the default tile: 2 * TP_X / TP)
 template <int N> struct FastLB<float2, N> {
-    static constexpr int ROW = 256, COL = 256, XT = 3 * 16 * 8, ROW_MIN = 3, COL_MIN = 3, X_MIN = 2;
+    static constexpr int ROW = 256, COL = 256, ROW_MIN = 3, COL_MIN = 3;
 };
 template <int N> struct FastLB<double2, N> {
-    static constexpr int ROW = 128, COL = 128, XT = 3 * 16 * 4, ROW_MIN = 3, COL_MIN = 3, X_MIN = 2;
+    static constexpr int ROW = 128, COL = 128, ROW_MIN = 3, COL_MIN = 3;
+};
+template <typename C, int TP> struct FastXLB {
+    static constexpr int XT = 3 * 16 * TP, X_MIN = 2 * FastTiles<C>::TP_X / TP;
 };
 
 // ---------------------------------------------------------------------------
@@ -120,12 +130,20 @@ __global__ void __launch_bounds__(FastLB<C, N>::ROW, FastLB<C, N>::ROW_MIN) kf_f
         const int i = (int)(row / op.ny), j = (int)(row - (long long)i * op.ny);
         const bool vrow = (s != 0 || i < op.nx - 1) && (s != 1 || j < op.ny - 1);
         C v[R1];
+        // the prologue's reads of a chunk of elements first, then its arithmetic and stores
+        constexpr int CH = R1 % 4 == 0 ? 4 : 1;
 #pragma unroll
-        for (int n1 = 0; n1 < R1; n1++) {
-            const int n = n2 + R2 * n1;
-            const bool valid = vrow && (s != 2 || n < N - 1);
-            C x = pro(s, row * N + n, valid);
-            v[n1] = valid ? x : czero<C>();
+        for (int c0 = 0; c0 < R1; c0 += CH) {
+            typename Pro::L ld[CH];
+#pragma unroll
+            for (int q = 0; q < CH; q++) ld[q] = pro.load(s, row * N + n2 + R2 * (c0 + q));
+#pragma unroll
+            for (int q = 0; q < CH; q++) {
+                const int n = n2 + R2 * (c0 + q);
+                const bool valid = vrow && (s != 2 || n < N - 1);
+                const C x = pro.apply(s, row * N + n, ld[q]);
+                v[c0 + q] = valid ? x : czero<C>();
+            }
         }
 #pragma unroll
         for (int h = 0; h < 2; h++) {
@@ -219,21 +237,46 @@ __global__ void __launch_bounds__(FastLB<C, N>::ROW, FastLB<C, N>::ROW_MIN) kf_i
         const bool vrow = (s != 0 || i < op.nx - 1) && (s != 1 || j < op.ny - 1);
         const long long sstep = s == 0 ? (long long)op.ny * N : (s == 1 ? (long long)N : 1LL);
         const R dc = op.dcoef[s];
+        const bool use_green = op.parts & 1, use_diag = op.parts & 2, use_mask = op.parts & 4;
+        // crop: the Green part y0 + W_2N^{-n} y1 of every element (frees the two halves)
+        C g[R1];
 #pragma unroll
-        for (int n1 = 0; n1 < R1; n1++) {
-            const int n = n2 + R2 * n1;
-            const long long idx = row * N + n;
-            C y = czero<C>();
-            if (!(op.parts & 4) || ((op.flags[idx] >> s) & 1)) {
-                if (op.parts & 1) y = cadd(y0[n1], cmulc(y1[n1], tw[n]));
-                if ((op.parts & 2) && vrow && (s != 2 || n < N - 1)) {
-                    const C ws = cadd(op.w[idx + sstep], op.w[idx]);
-                    C coef = mkc(-dc * ws.y, dc * ws.x);
-                    if (CONJ) coef = cconj(coef);
-                    y = cadd(y, cmul(coef, xin[(long long)s * op.a + idx]));
-                }
+        for (int n1 = 0; n1 < R1; n1++)
+            g[n1] = use_green ? cadd(y0[n1], cmulc(y1[n1], tw[n2 + R2 * n1])) : czero<C>();
+        // all reads of a chunk of elements (flags, contrast pair, diagonal source,
+        // the epilogue's vector) are issued before its arithmetic and stores;
+        // the selections below give the results of the branchy form bit for bit
+        constexpr int CH = R1 % 4 == 0 ? 4 : 1;
+#pragma unroll
+        for (int c0 = 0; c0 < R1; c0 += CH) {
+            unsigned char fl[CH];
+            C wa[CH], wb[CH], xv[CH], pv[CH];
+#pragma unroll
+            for (int q = 0; q < CH; q++) {
+                const int n = n2 + R2 * (c0 + q);
+                const long long idx = row * N + n;
+                const bool dv = vrow && (s != 2 || n < N - 1);
+                fl[q] = op.flags[idx];
+                wa[q] = op.w[idx];
+                wb[q] = op.w[dv ? idx + sstep : idx];
+                xv[q] = xin[(long long)s * op.a + idx];
+                pv[q] = epi.pre(s, idx);
             }
-            epi(s, idx, y, acc);
+#pragma unroll
+            for (int q = 0; q < CH; q++) {
+                const int n1 = c0 + q;
+                const int n = n2 + R2 * n1;
+                const long long idx = row * N + n;
+                const bool dv = use_diag && vrow && (s != 2 || n < N - 1);
+                C y = g[n1];
+                const C ws = cadd(wb[q], wa[q]);
+                C coef = mkc(-dc * ws.y, dc * ws.x);
+                if (CONJ) coef = cconj(coef);
+                const C yd = cadd(y, cmul(coef, xv[q]));
+                y = dv ? yd : y;
+                y = (!use_mask || ((fl[q] >> s) & 1)) ? y : czero<C>();
+                epi.put(s, idx, y, acc, pv[q]);
+            }
         }
     }
     if constexpr (Epi::K > 0) block_reduce_store<KA>(acc, partial, (long long)blockIdx.y * gridDim.x + blockIdx.x);
@@ -342,13 +385,13 @@ __global__ void __launch_bounds__(FastLB<C, N>::COL, FastLB<C, N>::COL_MIN) kf_i
 // then E[s][h][k1][k2][tx] (spectra) then E[s][h][k1][n2][tx] (inverse).
 // Thread roles: steps A/A' (tx, s, n2); step B / multiply / B' (tx, h, k1).
 // ---------------------------------------------------------------------------
-template <typename C, int N, bool CONJ>
-__global__ void __launch_bounds__(FastLB<C, N>::XT, FastLB<C, N>::X_MIN) kf_x_spectral(OpDev<C> op) {
+template <typename C, int N, bool CONJ, int TP>
+__global__ void __launch_bounds__(FastXLB<C, TP>::XT, FastXLB<C, TP>::X_MIN) kf_x_spectral(OpDev<C> op) {
     if (gate_closed(op.gate)) return;
     using R = typename real_of<C>::type;
-    constexpr int R1 = FastPlan<N>::R1, R2 = FastPlan<N>::R2, TP = FastTiles<C>::TP_X;
+    constexpr int R1 = FastPlan<N>::R1, R2 = FastPlan<N>::R2;
     constexpr int L = R1 > R2 ? R1 : R2;
-    constexpr int KS = fast_x_kstride<C, N>();  // stride of k1 (R2*TP + TP padding)
+    constexpr int KS = fast_x_kstride<C, N, TP>();  // stride of k1 (R2*TP + TP padding)
     constexpr int HS = R1 * KS, SS = 2 * HS;
     C* tw;
     C* E = fast_smem<C, N>(op.ax[0].tw, tw);
@@ -450,8 +493,8 @@ __global__ void __launch_bounds__(FastLB<C, N>::XT, FastLB<C, N>::X_MIN) kf_x_sp
     }
 }
 
-template <typename C, int N> constexpr int fast_x_threads() {
-    return 3 * (FastPlan<N>::R1 > FastPlan<N>::R2 ? FastPlan<N>::R1 : FastPlan<N>::R2) * FastTiles<C>::TP_X;
+template <typename C, int N, int TP = FastTiles<C>::TP_X> constexpr int fast_x_threads() {
+    return 3 * (FastPlan<N>::R1 > FastPlan<N>::R2 ? FastPlan<N>::R1 : FastPlan<N>::R2) * TP;
 }
 
 }  // namespace vie

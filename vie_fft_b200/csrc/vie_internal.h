@@ -46,6 +46,7 @@ std::vector<int> axis_perm(const AxisPlan& pl);
 struct TileCfg {
     int tz = 0, tc = 0, tx = 0;
     int fast[3] = {-1, -1, -1};  // per axis: 1 register four-step kernels, 0 generic, -1 automatic
+    int xalt = 0;                // register x pass with the half pencil tile
 };
 
 // Operator state for one arithmetic precision.  Owns its tables, the Green

@@ -490,15 +490,22 @@ __global__ void k_fold_correction(double2* __restrict__ x64, float2* __restrict_
 // ---------------------------------------------------------------------------
 // prologue / epilogue functors of the fused BiCGSTAB and refinement
 // ---------------------------------------------------------------------------
+// Each prologue has load(s, idx) (every global read of one element, issued
+// before any store so a chunk of elements can be loaded together) and
+// apply(s, idx, loaded) (arithmetic and stores); each epilogue has pre(s, idx)
+// (the vector it reads) and put(s, idx, y, acc, pre).  operator() chains them
+// for kernels that work element by element.
 template <typename C> struct ProCopyWrite {  // p = r
     const C* __restrict__ r;
     C* __restrict__ p;
     long long a;
-    __device__ __forceinline__ C operator()(int s, long long idx, bool) const {
-        const C v = r[s * a + idx];
-        p[s * a + idx] = v;
-        return v;
+    struct L { C r; };
+    __device__ __forceinline__ L load(int s, long long idx) const { return L{r[s * a + idx]}; }
+    __device__ __forceinline__ C apply(int s, long long idx, const L& l) const {
+        p[s * a + idx] = l.r;
+        return l.r;
     }
+    __device__ __forceinline__ C operator()(int s, long long idx, bool) const { return apply(s, idx, load(s, idx)); }
 };
 template <typename C> struct ProBicgP {  // p = r + beta (p - omega v)
     const C* __restrict__ r;
@@ -506,13 +513,17 @@ template <typename C> struct ProBicgP {  // p = r + beta (p - omega v)
     const C* __restrict__ v;
     const double2* __restrict__ S;
     long long a;
-    __device__ __forceinline__ C operator()(int s, long long idx, bool) const {
-        const C beta = from_d2<C>(S[S_BETA]), omega = from_d2<C>(S[S_OMEGA]);
+    struct L { C r, p, v, beta, omega; };
+    __device__ __forceinline__ L load(int s, long long idx) const {
         const long long o = s * a + idx;
-        const C pv = cadd(r[o], cmul(beta, csub(p[o], cmul(omega, v[o]))));
-        p[o] = pv;
+        return L{r[o], p[o], v[o], from_d2<C>(S[S_BETA]), from_d2<C>(S[S_OMEGA])};
+    }
+    __device__ __forceinline__ C apply(int s, long long idx, const L& l) const {
+        const C pv = cadd(l.r, cmul(l.beta, csub(l.p, cmul(l.omega, l.v))));
+        p[s * a + idx] = pv;
         return pv;
     }
+    __device__ __forceinline__ C operator()(int s, long long idx, bool) const { return apply(s, idx, load(s, idx)); }
 };
 template <typename C> struct ProBicgS {  // s = r - alpha v
     const C* __restrict__ r;
@@ -520,23 +531,30 @@ template <typename C> struct ProBicgS {  // s = r - alpha v
     C* __restrict__ sv;
     const double2* __restrict__ S;
     long long a;
-    __device__ __forceinline__ C operator()(int s, long long idx, bool) const {
-        const C alpha = from_d2<C>(S[S_ALPHA]);
+    struct L { C r, v, alpha; };
+    __device__ __forceinline__ L load(int s, long long idx) const {
         const long long o = s * a + idx;
-        const C x = csub(r[o], cmul(alpha, v[o]));
-        sv[o] = x;
+        return L{r[o], v[o], from_d2<C>(S[S_ALPHA])};
+    }
+    __device__ __forceinline__ C apply(int s, long long idx, const L& l) const {
+        const C x = csub(l.r, cmul(l.alpha, l.v));
+        sv[s * a + idx] = x;
         return x;
     }
+    __device__ __forceinline__ C operator()(int s, long long idx, bool) const { return apply(s, idx, load(s, idx)); }
 };
 template <typename C> struct EpiDotB {  // store y; acc conj(b) y
     static constexpr int K = 1;
     C* __restrict__ y;
     const C* __restrict__ b;
     long long a;
+    __device__ __forceinline__ C pre(int s, long long idx) const { return b[s * a + idx]; }
+    __device__ __forceinline__ void put(int s, long long idx, C v, double2* acc, C bv) const {
+        y[s * a + idx] = v;
+        acc_dotc(acc[0], bv, v);
+    }
     __device__ __forceinline__ void operator()(int s, long long idx, C v, double2* acc) const {
-        const long long o = s * a + idx;
-        y[o] = v;
-        acc_dotc(acc[0], b[o], v);
+        put(s, idx, v, acc, pre(s, idx));
     }
 };
 template <typename C> struct EpiDotTS {  // store t; acc conj(t) s, conj(t) t
@@ -544,20 +562,27 @@ template <typename C> struct EpiDotTS {  // store t; acc conj(t) s, conj(t) t
     C* __restrict__ y;
     const C* __restrict__ sv;
     long long a;
-    __device__ __forceinline__ void operator()(int s, long long idx, C v, double2* acc) const {
-        const long long o = s * a + idx;
-        y[o] = v;
-        acc_dotc(acc[0], v, sv[o]);
+    __device__ __forceinline__ C pre(int s, long long idx) const { return sv[s * a + idx]; }
+    __device__ __forceinline__ void put(int s, long long idx, C v, double2* acc, C svv) const {
+        y[s * a + idx] = v;
+        acc_dotc(acc[0], v, svv);
         acc_dotc(acc[1], v, v);
+    }
+    __device__ __forceinline__ void operator()(int s, long long idx, C v, double2* acc) const {
+        put(s, idx, v, acc, pre(s, idx));
     }
 };
 template <typename C> struct EpiNorm {  // store y; acc ||y||^2
     static constexpr int K = 1;
     C* __restrict__ y;
     long long a;
-    __device__ __forceinline__ void operator()(int s, long long idx, C v, double2* acc) const {
+    __device__ __forceinline__ C pre(int, long long) const { return czero<C>(); }
+    __device__ __forceinline__ void put(int s, long long idx, C v, double2* acc, C) const {
         y[s * a + idx] = v;
         acc_dotc(acc[0], v, v);
+    }
+    __device__ __forceinline__ void operator()(int s, long long idx, C v, double2* acc) const {
+        put(s, idx, v, acc, czero<C>());
     }
 };
 template <typename C> struct EpiDotU {  // store y; acc y^T u (unconjugated)
@@ -565,10 +590,13 @@ template <typename C> struct EpiDotU {  // store y; acc y^T u (unconjugated)
     C* __restrict__ y;
     const C* __restrict__ u;
     long long a;
+    __device__ __forceinline__ C pre(int s, long long idx) const { return u[s * a + idx]; }
+    __device__ __forceinline__ void put(int s, long long idx, C v, double2* acc, C uv) const {
+        y[s * a + idx] = v;
+        acc_dotu(acc[0], v, uv);
+    }
     __device__ __forceinline__ void operator()(int s, long long idx, C v, double2* acc) const {
-        const long long o = s * a + idx;
-        y[o] = v;
-        acc_dotu(acc[0], v, u[o]);
+        put(s, idx, v, acc, pre(s, idx));
     }
 };
 template <typename C> struct EpiResidual {  // r = b - y; acc ||r||^2
@@ -576,11 +604,14 @@ template <typename C> struct EpiResidual {  // r = b - y; acc ||r||^2
     C* __restrict__ r;
     const C* __restrict__ b;
     long long a;
-    __device__ __forceinline__ void operator()(int s, long long idx, C v, double2* acc) const {
-        const long long o = s * a + idx;
-        const C rv = csub(b[o], v);
-        r[o] = rv;
+    __device__ __forceinline__ C pre(int s, long long idx) const { return b[s * a + idx]; }
+    __device__ __forceinline__ void put(int s, long long idx, C v, double2* acc, C bv) const {
+        const C rv = csub(bv, v);
+        r[s * a + idx] = rv;
         acc_dotc(acc[0], rv, rv);
+    }
+    __device__ __forceinline__ void operator()(int s, long long idx, C v, double2* acc) const {
+        put(s, idx, v, acc, pre(s, idx));
     }
 };
 

@@ -88,17 +88,23 @@ int launch_fast_y(Operator<T>& op, bool forward, cudaStream_t st, Error& err) {
     return VIE_OK;
 }
 
+template <typename T, int N, int TP>
+int launch_fast_x_tp(Operator<T>& op, bool conj, cudaStream_t st, Error& err) {
+    using C = cplx_t<T>;
+    constexpr size_t smem = fast_smem_x<C, N, TP>();
+    dim3 grid(ceil_div(2 * op.dev.nz, TP), 2 * op.dev.ny);
+    auto kf = conj ? kf_x_spectral<C, N, true, TP> : kf_x_spectral<C, N, false, TP>;
+    VIE_CUDA_TRY(ensure_smem(kf, smem), err);
+    kf<<<grid, fast_x_threads<C, N, TP>(), smem, st>>>(op.dev);
+    count_launch();
+    return VIE_OK;
+}
+// the x pass with the operator's tile choice (OpDev::xalt: 0 default, 1 half)
 template <typename T, int N>
 int launch_fast_x(Operator<T>& op, bool conj, cudaStream_t st, Error& err) {
     using C = cplx_t<T>;
-    constexpr int TP = FastTiles<C>::TP_X;
-    constexpr size_t smem = fast_smem_x<C, N>();
-    dim3 grid(ceil_div(2 * op.dev.nz, TP), 2 * op.dev.ny);
-    auto kf = conj ? kf_x_spectral<C, N, true> : kf_x_spectral<C, N, false>;
-    VIE_CUDA_TRY(ensure_smem(kf, smem), err);
-    kf<<<grid, fast_x_threads<C, N>(), smem, st>>>(op.dev);
-    count_launch();
-    return VIE_OK;
+    if (op.dev.xalt) return launch_fast_x_tp<T, N, FastTiles<C>::TP_X / 2>(op, conj, st, err);
+    return launch_fast_x_tp<T, N, FastTiles<C>::TP_X>(op, conj, st, err);
 }
 
 #define VIE_FAST_SWITCH(n, CALL)                                   \

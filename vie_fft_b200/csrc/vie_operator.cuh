@@ -61,6 +61,7 @@ template <typename C> struct OpDev {
     const C* w;                // per voxel 1/(eps-1)
     const unsigned char* flags;  // bit0 Flag_X, bit1 Flag_Y, bit2 Flag_Z
     int fast[3];               // axis uses the register four-step kernels (half-natural slots)
+    int xalt;                  // register x pass with the alternative (half) pencil tile
     int parts;                 // VIE_PART_* bits: Green blocks, diagonal term, edge mask
     typename real_of<C>::type kappa[3];   // k0^2 delta_f
     typename real_of<C>::type dcoef[3];   // -delta_f Z0 / (2 k0)
@@ -333,9 +334,14 @@ __global__ void __launch_bounds__(kThreads) k_inv_z(OpDev<C> op, const C* __rest
 // ---------------------------------------------------------------------------
 // prologue / epilogue functors
 // ---------------------------------------------------------------------------
+// prologue / epilogue interface: load/apply and pre/put split the global
+// reads from the arithmetic and the stores (see the Krylov functors)
 template <typename C> struct ProCopy {
     const C* __restrict__ x;
     long long a;
+    struct L { C x; };
+    __device__ __forceinline__ L load(int s, long long idx) const { return L{x[s * a + idx]}; }
+    __device__ __forceinline__ C apply(int, long long, const L& l) const { return l.x; }
     __device__ __forceinline__ C operator()(int s, long long idx, bool) const { return x[s * a + idx]; }
 };
 
@@ -343,6 +349,8 @@ template <typename C> struct EpiStore {
     static constexpr int K = 0;
     C* __restrict__ y;
     long long a;
+    __device__ __forceinline__ C pre(int, long long) const { return czero<C>(); }
+    __device__ __forceinline__ void put(int s, long long idx, C v, double2*, C) const { y[s * a + idx] = v; }
     __device__ __forceinline__ void operator()(int s, long long idx, C v, double2*) const { y[s * a + idx] = v; }
 };
 

@@ -59,7 +59,7 @@ std::string serialize(const std::string& key, const Sched& s) {
         o << ' ' << s.t.fast[ax] << ' ' << tile[ax] << ' ' << s.plan[ax].nst;
         for (int i = 0; i < s.plan[ax].nst; i++) o << ' ' << s.plan[ax].rad[i];
     }
-    o << ' ' << s.ms;
+    o << ' ' << s.t.xalt << ' ' << s.ms;
     return o.str();
 }
 
@@ -90,7 +90,7 @@ void load_file_locked() {
             s.plan[ax].n = prod;
             ok = ok && prod == k[1 + ax];
         }
-        ok = ok && (in >> s.ms);
+        ok = ok && (in >> s.t.xalt >> s.ms) && (s.t.xalt == 0 || s.t.xalt == 1);
         if (!ok) continue;
         s.t.tx = tile[0];
         s.t.tc = tile[1];
@@ -185,7 +185,12 @@ template <typename T> int tune_one(vie_ctx* ctx, Operator<T>& op, Sched& best, s
         if (fast_length(n[ax])) {
             Sched s = best;
             s.t.fast[ax] = 1;
+            s.ms = 0.f;  // measured below
             cands.push_back(s);
+            if (ax == 0) {  // the register x pass with the half pencil tile
+                s.t.xalt = 1;
+                cands.push_back(s);
+            }
         }
         Sched bestg;
         float bestg_ms = 1e30f;
@@ -233,7 +238,8 @@ template <typename T> int tune_one(vie_ctx* ctx, Operator<T>& op, Sched& best, s
         const int tl[3] = {best.t.tx, best.t.tc, best.t.tz};
         for (int ax = 0; ax < 3; ax++) {
             o << ' ' << nm[ax] << '=';
-            if (best.t.fast[ax] == 1 || (best.t.fast[ax] < 0 && fast_length(n[ax]))) o << "fast";
+            if (best.t.fast[ax] == 1 || (best.t.fast[ax] < 0 && fast_length(n[ax])))
+                o << "fast" << (ax == 0 && best.t.xalt ? "/half-tile" : "");
             else o << "generic[" << plan_str(best.plan[ax]) << "]/t" << tl[ax];
         }
         report = o.str();
