@@ -216,7 +216,8 @@ def run_gpu(args, rank, world, local_rank):
     if world > 1:
         # replicas: each rank solves its own wavelength of the same geometry
         from vie_fft_b200 import geometry as G
-        w.k0 = G.k0_of(w.meta["wavelength_nm"] + 5.0 * rank)
+        from vie_fft_b200.replicas import replica_wavelength
+        w.k0 = G.k0_of(replica_wavelength(w.meta["wavelength_nm"], rank))
     c = V.Context(*w.shape, *w.d, w.k0, device=local_rank)
     c.set_flags(w.flags)
     if w.eps_voxel is not None:
@@ -286,11 +287,8 @@ def run_gpu(args, rank, world, local_rank):
     launches = V.launch_count() - launches0
     clocks = sampler.stop() if sampler else None
     ms = ev0.elapsed_time(ev1) / args.steps
-    t_all = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if dist is not None:
-        dist.all_reduce(t_all, op=dist.ReduceOp.MAX)
-    ms_max = float(t_all.item())
-    value = world * 1e3 / ms_max
+    from vie_fft_b200.replicas import throughput
+    value, ms_max = throughput(1.0, ms, device="cuda")
     x_mixed = c.solution()
 
     # ---- FP64 reference solve of the same system (speed-up and accuracy)
@@ -356,10 +354,8 @@ def run_gpu(args, rank, world, local_rank):
         f1.synchronize()
         wall = (time.perf_counter() - tw0) / args.e2e_steps
         ms_e2e = f0.elapsed_time(f1) / args.e2e_steps
-        te = torch.tensor([ms_e2e], dtype=torch.float64, device="cuda")
-        if dist is not None:
-            dist.all_reduce(te, op=dist.ReduceOp.MAX)
-        e2e = {"value": world * 1e3 / float(te.item()), "unit": "solves/s",
+        e2e_value, _ = throughput(1.0, ms_e2e, device="cuda")
+        e2e = {"value": e2e_value, "unit": "solves/s",
                "h2d_bytes_per_step": int(h_rhs.numel() * 16), "d2h_bytes_per_step": int(h_x.numel() * 16),
                "wall_ms_per_step": wall * 1e3}
 
@@ -449,7 +445,9 @@ def run_gpu_batch(args, rank, world, local_rank):
     from vie_fft_b200 import post
 
     torch.cuda.set_device(local_rank)
-    ws, desc = batch_workloads(args.workload)
+    from vie_fft_b200.replicas import shard, throughput
+    ws_all, desc = batch_workloads(args.workload)
+    ws = shard(ws_all, rank, world)  # replicas: each rank solves its share of the instances
     t0 = time.perf_counter()
     ctxs = []
     for w in ws:
@@ -472,7 +470,9 @@ def run_gpu_batch(args, rank, world, local_rank):
         secs.append(res[0].info["seconds"])
     launches = V.launch_count() - launches0
     clocks = sampler.stop() if sampler else None
-    t_mixed = statistics.median(secs)
+    t_mixed_local = statistics.median(secs)
+    value_all, ms_max = throughput(len(ws), t_mixed_local * 1e3, device="cuda")
+    t_mixed = ms_max / 1e3
     x_mixed = [c.solution() for c in ctxs]
     r64 = V.solve_batch(ctxs, "bicgstab", tol=TOL, precision=V.PREC_FP64, copy=True, raise_errors=False)
     t64 = r64[0].info["seconds"]
@@ -487,10 +487,11 @@ def run_gpu_batch(args, rank, world, local_rank):
     it64 = [r.info["iterations"] for r in r64]
     line = {
         "metric": "batched instances/s to rel-res 1e-8 (FP32 inner / FP64 refine, one graph launch per batch)",
-        "value": n / t_mixed, "unit": "instances/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "value": value_all, "unit": "instances/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": t_mixed * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "c64 inner + c128 refine", "data": "synthetic",
-        "config": {"workload": desc, "instances": n, "solver": "bicgstab", "tol": TOL,
+        "config": {"workload": desc, "instances": len(ws_all), "instances_per_rank": n, "solver": "bicgstab",
+                   "tol": TOL, "parallelism": f"replicas x{world}" if world > 1 else "single",
                    "voxels_total": int(sum(w.a for w in ws))},
         "fp64": {"instances_per_s": n / t64, "s_per_batch": t64, "iterations_min_max": [min(it64), max(it64)]},
         "speedup_mixed_vs_fp64": t64 / t_mixed,
