@@ -189,6 +189,34 @@ VIE_API int vie_solve_batch(vie_ctx* const* ctxs, int n, const vie_solve_params*
    info_fwd / info_adj (may be NULL) receive the two solves' counts. */
 VIE_API int vie_power_grad(vie_ctx* ctx, const unsigned char* edge_mask, const vie_solve_params* p, double* power,
                            double* grad, vie_solve_info* info_fwd, vie_solve_info* info_adj);
+/* Geometry on the GPU (GetMaterial / GetFlag, Model.h:305-398, without host
+   label evaluation).  A scene is a list of primitives in priority order: the
+   label of a point is that of the first primitive holding it whose parent
+   (another primitive of the list, or -1) holds it too, else 0 (air): e.g. the
+   reference's layered model lists its spheres first with the spacer box as
+   parent, then the spacer box, then the active box.  The primitive
+   tests are the reference's forms of Model_Identifier (Model.h:215-300):
+   VIE_PRIM_SPHERE sqrt(|p - c|^2) <= r (its one-sphere model), VIE_PRIM_SPHERE_F32
+   float(|p - c|^2) < float(r^2) (the sphere loop of its layered model) and
+   VIE_PRIM_BOX |p_i - c_i| < h_i on every axis (its layers).  Coordinates in
+   the grid's units, origin at the grid corner.  Sets the edge flags and the
+   permittivity from the table (as vie_set_flags + vie_set_material) and, when
+   material_out != NULL, returns the labels (a bytes).  At most 256 primitives. */
+#define VIE_PRIM_SPHERE 1
+#define VIE_PRIM_SPHERE_F32 2
+#define VIE_PRIM_BOX 3
+typedef struct {
+    int kind;     /* VIE_PRIM_* */
+    int label;    /* material index 0..255 */
+    int parent;   /* index of another primitive that must also hold the point, or -1 */
+    int pad;
+    double c[3];  /* centre */
+    double r;     /* sphere radius */
+    double h[3];  /* box half-widths */
+} vie_primitive;
+VIE_API int vie_set_geometry_scene(vie_ctx* ctx, const vie_primitive* prims, int n, const double* eps_re,
+                                   const double* eps_im, int n_materials, uint8_t* material_out);
+
 /* Post-processing of the last solution on the GPU (the field stays on the
    device).  vie_farfield1 replaces FarField1 (NearFar.h:16-109): Forward_RCS
    for the incidence angles theta, phi, psi (degrees).  vie_farfield2 replaces

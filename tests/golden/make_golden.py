@@ -15,6 +15,8 @@ Fixtures
   c1_sphere.npz      the 32^3 silver-sphere BiCGSTAB solve to 1e-6: step
                      count, solution on the flagged edges, FarField1 and
                      NearField outputs
+  geometry.npz       the reference's GetMaterial / GetFlag of its one-sphere
+                     model (Model_Identifier) on a cubic and a non-cubic grid
   post_ops.npz       FarField1, FarField2 (RCS) and NearField outputs of the
                      reference on seeded currents of the small cases
   dropin_blocks.npz  X/Y/Z_FFT rows, L_DC_Dq, L_Dq, L??_DO (and conjugate
@@ -117,6 +119,25 @@ def make_c1():
                         forward_rcs=fwd, ext_over_cs=ext, metal_abs_over_cs=metal)
 
 
+GEOMETRY_CASES = [
+    # (shape, d, dia, box)
+    ((32, 32, 32), (0.0125, 0.0125, 0.0125), 0.36, (0.4, 0.4, 0.4)),
+    ((20, 24, 16), (0.011, 0.01, 0.013), 0.18, (0.22, 0.24, 0.2)),
+]
+
+
+def make_geometry():
+    out = {}
+    for idx, (shape, d, dia, box) in enumerate(GEOMETRY_CASES):
+        g = O.Grid(*shape, *d, G.k0_of(500.0))
+        R = O.Reference(g, EPS_TABLE)
+        R.sphere_geometry(dia, *box)
+        m, f = R.get_geometry()
+        out[f"material{idx}"], out[f"flags{idx}"] = m, f
+        R.release()
+    np.savez_compressed(os.path.join(OUT, "geometry.npz"), **out)
+
+
 def make_post_ops():
     out = {}
     for idx in range(len(SMALL)):
@@ -208,13 +229,15 @@ def make_dropin_program():
 
 if __name__ == "__main__":
     import sys as _sys
-    which = _sys.argv[1:] or ["ops", "solves", "c1", "post", "blocks", "program"]
+    which = _sys.argv[1:] or ["ops", "solves", "c1", "geometry", "post", "blocks", "program"]
     if "ops" in which:
         make_small_ops()
     if "solves" in which:
         make_small_solves()
     if "c1" in which:
         make_c1()
+    if "geometry" in which:
+        make_geometry()
     if "post" in which:
         make_post_ops()
     if "blocks" in which:

@@ -58,6 +58,14 @@ class VieSolveParams(ctypes.Structure):
                 ("verbose", ctypes.c_int), ("true_residual", ctypes.c_int)]
 
 
+class ViePrimitive(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int), ("label", ctypes.c_int), ("parent", ctypes.c_int), ("pad", ctypes.c_int),
+                ("c", ctypes.c_double * 3), ("r", ctypes.c_double), ("h", ctypes.c_double * 3)]
+
+
+PRIM_SPHERE, PRIM_SPHERE_F32, PRIM_BOX = 1, 2, 3
+
+
 class VieSolveInfo(ctypes.Structure):
     _fields_ = [("steps", ctypes.c_int), ("iterations", ctypes.c_int), ("outer", ctypes.c_int),
                 ("matvecs_fp64", ctypes.c_int), ("matvecs_fp32", ctypes.c_int), ("relres", ctypes.c_double),
@@ -93,6 +101,7 @@ def lib():
         L.vie_set_material.argtypes = [_vp, _up, _dp, _dp, ctypes.c_int]
         L.vie_set_eps.argtypes = [_vp, _dp]
         L.vie_set_flags.argtypes = [_vp, _up, _up, _up]
+        L.vie_set_geometry_scene.argtypes = [_vp, P(ViePrimitive), ctypes.c_int, _dp, _dp, ctypes.c_int, _up]
         L.vie_green.argtypes = [_vp]
         L.vie_green_spectrum.argtypes = [_vp, _dp]
         L.vie_incident.argtypes = [_vp, ctypes.c_double, ctypes.c_double, ctypes.c_double, _dp]
@@ -189,6 +198,27 @@ class Context:
     def set_eps(self, eps):
         e = _c128(eps, self.shape)
         self._check(self._L.vie_set_eps(self._h, _p(e)))
+
+    def set_scene(self, prims, eps_table):
+        """Material labels and edge flags from an analytic scene, evaluated on the
+        GPU (``vie_set_geometry_scene``).  prims: dicts with kind (PRIM_*), label,
+        c (centre), r (sphere radius), h (box half-widths), parent (-1).
+        Returns the material labels (nx, ny, nz) uint8."""
+        arr = (ViePrimitive * max(len(prims), 1))()
+        for q, p in enumerate(prims):
+            arr[q].kind = int(p["kind"])
+            arr[q].label = int(p["label"])
+            arr[q].parent = int(p.get("parent", -1))
+            for t in range(3):
+                arr[q].c[t] = float(p.get("c", (0, 0, 0))[t])
+                arr[q].h[t] = float(p.get("h", (0, 0, 0))[t])
+            arr[q].r = float(p.get("r", 0.0))
+        t = np.asarray(eps_table, np.complex128)
+        re, im = np.ascontiguousarray(t.real), np.ascontiguousarray(t.imag)
+        mat = np.zeros(self.shape, np.uint8)
+        ptr = ctypes.cast(arr, ctypes.POINTER(ViePrimitive))
+        self._check(self._L.vie_set_geometry_scene(self._h, ptr, len(prims), _p(re), _p(im), len(t), _p(mat, _up)))
+        return mat
 
     def set_flags(self, flags):
         f = np.ascontiguousarray(flags, np.uint8)

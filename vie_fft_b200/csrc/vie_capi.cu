@@ -15,6 +15,8 @@ int incident_compute(vie_ctx* ctx, double theta, double phi, double psi, double2
 int solve_driver(vie_ctx* ctx, const vie_solve_params* prm, vie_solve_info* info);
 int solve_batch_driver(vie_ctx* const* ctxs, int n, const vie_solve_params* prm, vie_solve_info* infos);
 void tune_apply_cached(vie_ctx* ctx);
+int scene_driver(vie_ctx* ctx, const vie_primitive* prims, int n, unsigned char* material_out);
+int scene_check(const vie_primitive* prims, int n);
 int farfield1_driver(vie_ctx* ctx, double theta, double phi, double psi, double* fwd);
 int farfield2_driver(vie_ctx* ctx, double phi, double* rcs_theta, double* rcs_phi);
 int nearfield_driver(vie_ctx* ctx, const unsigned char* material, double* out3);
@@ -199,6 +201,27 @@ int vie_set_material(vie_ctx* ctx, const uint8_t* material, const double* eps_re
         eps[2 * v + 1] = eps_im[m];
     }
     return vie_set_eps(ctx, eps.data());
+}
+
+int vie_set_geometry_scene(vie_ctx* ctx, const vie_primitive* prims, int n, const double* eps_re,
+                           const double* eps_im, int n_materials, uint8_t* material_out) {
+    if (check_ctx(ctx) || !eps_re || !eps_im || n_materials < 1 || n_materials > 256) return VIE_ERR_ARG;
+    if (scene_check(prims, n)) return ctx->set_error(VIE_ERR_ARG, "invalid scene primitive (kind, label or parent)");
+    for (int q = 0; q < n; q++)
+        if (prims[q].label >= n_materials) return ctx->set_error(VIE_ERR_ARG, "scene label outside the table");
+    cudaSetDevice(ctx->device);
+    std::vector<uint8_t> mat((size_t)ctx->a);
+    int rc = scene_driver(ctx, prims, n, mat.data());
+    if (rc) return rc;
+    ctx->have_flags = true;
+    if ((rc = vie_set_material(ctx, mat.data(), eps_re, eps_im, n_materials))) return rc;
+    if ((rc = ensure_operators(ctx))) return rc;
+    if (ctx->have_green) {
+        rc = ctx->op64.set_green(ctx->d_green, ctx->k0, ctx->stream, ctx->err);
+        if (!rc) rc = ctx->op32.set_green(ctx->d_green, ctx->k0, ctx->stream, ctx->err);
+    }
+    if (!rc && material_out) std::memcpy(material_out, mat.data(), (size_t)ctx->a);
+    return rc;
 }
 
 int vie_set_flags(vie_ctx* ctx, const uint8_t* fx, const uint8_t* fy, const uint8_t* fz) {
