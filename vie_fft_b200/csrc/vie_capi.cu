@@ -50,6 +50,8 @@ TileCfg tiles_from_env() {
         int a = 0, b = 0, c = 0;
         if (std::sscanf(s, "%d,%d,%d", &a, &b, &c) == 3) { t.tz = a; t.tc = b; t.tx = c; }
     }
+    // VIE_XTILE=1: the register x pass with the half pencil tile (otherwise the autotuner decides)
+    if (const char* x = std::getenv("VIE_XTILE")) t.xalt = std::atoi(x) == 1 ? 1 : 0;
     return t;
 }
 
