@@ -47,9 +47,11 @@ def test_small_cases_match_reference(idx):
 
 # shapes cover the generic kernels (odd and prime lengths) and every length
 # with register four-step kernels: 16..256 powers of two and the mixed-radix
-# 24 (8x3), 40 (8x5), 48 (8x6), 56 (8x7), 72 (8x9), 80 (16x5), 88 (8x11), 96 (16x6)
+# 24 (8x3), 40 (8x5), 48 (8x6), 56 (8x7), 72 (8x9), 80 (16x5), 88 (8x11), 96 (16x6),
+# 112 (16x7), 120 (8x15), 144 (16x9), 160 (16x10), 176 (16x11), 192 (16x12)
 @pytest.mark.parametrize("shape", [(24, 20, 16), (31, 17, 13), (48, 40, 56), (9, 7, 5), (2, 2, 2), (16, 3, 64),
-                                   (72, 88, 16), (96, 24, 80), (32, 72, 40)])
+                                   (72, 88, 16), (96, 24, 80), (32, 72, 40), (112, 120, 16), (144, 16, 160),
+                                   (176, 16, 192)])
 def test_matvec_fp64_matches_oracle(shape):
     rng = np.random.default_rng(sum(shape))
     d = (0.01, 0.012, 0.011)
@@ -71,7 +73,8 @@ def _torch():
     return torch
 
 
-@pytest.mark.parametrize("shape", [(24, 20, 16), (31, 17, 13), (48, 40, 56), (72, 88, 16), (96, 24, 80)])
+@pytest.mark.parametrize("shape", [(24, 20, 16), (31, 17, 13), (48, 40, 56), (72, 88, 16), (96, 24, 80),
+                                   (112, 120, 16), (176, 16, 192)])
 def test_matvec_fp32_matches_oracle(shape):
     torch = _torch()
     rng = np.random.default_rng(5)

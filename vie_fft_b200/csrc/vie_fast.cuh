@@ -26,7 +26,13 @@ template <int N> struct FastPlan { static constexpr bool ok = false; static cons
 #define VIE_FAST_PLAN(NN, A, B) \
     template <> struct FastPlan<NN> { static constexpr bool ok = true; static constexpr int R1 = A, R2 = B; };
 VIE_FAST_PLAN(256, 16, 16)
+VIE_FAST_PLAN(192, 16, 12)
+VIE_FAST_PLAN(176, 16, 11)
+VIE_FAST_PLAN(160, 16, 10)
+VIE_FAST_PLAN(144, 16, 9)
 VIE_FAST_PLAN(128, 16, 8)
+VIE_FAST_PLAN(120, 8, 15)
+VIE_FAST_PLAN(112, 16, 7)
 VIE_FAST_PLAN(96, 16, 6)
 VIE_FAST_PLAN(88, 8, 11)
 VIE_FAST_PLAN(80, 16, 5)
@@ -40,7 +46,9 @@ VIE_FAST_PLAN(24, 8, 3)
 VIE_FAST_PLAN(16, 4, 4)
 #undef VIE_FAST_PLAN
 // the axis lengths with register four-step kernels (one case per FastPlan above)
-#define VIE_FAST_LENGTHS(X) X(256) X(128) X(96) X(88) X(80) X(72) X(64) X(56) X(48) X(40) X(32) X(24) X(16)
+#define VIE_FAST_LENGTHS(X) \
+    X(256) X(192) X(176) X(160) X(144) X(128) X(120) X(112) X(96) X(88) X(80) X(72) X(64) X(56) X(48) X(40) X(32) \
+    X(24) X(16)
 
 inline bool fast_length(int n) {
 #define VIE_FL_CASE(NN) if (n == NN) return true;
@@ -182,9 +190,11 @@ __global__ void __launch_bounds__(FastLB<C, N>::ROW, FastLB<C, N>::ROW_MIN) kf_f
 // I1 (row pass): inverse z, crop, diagonal term, mask, epilogue.
 // E layout: E[h][row][n2][k1], n2 stride R1 + 1.
 // ---------------------------------------------------------------------------
-template <typename C, int N, bool CONJ, class Epi>
+// (conj: the adjoint operator's diagonal coefficient; a run-time flag, the
+// two modes differ by one conjugation)
+template <typename C, int N, class Epi>
 __global__ void __launch_bounds__(FastLB<C, N>::ROW, FastLB<C, N>::ROW_MIN) kf_inv_z(OpDev<C> op, const C* __restrict__ xin, Epi epi,
-                                                double2* __restrict__ partial) {
+                                                double2* __restrict__ partial, int conj) {
     if (gate_closed(op.gate)) return;
     using R = typename real_of<C>::type;
     constexpr int R1 = FastPlan<N>::R1, R2 = FastPlan<N>::R2, L = fast_lanes<C, N>(), ROWS = fast_rows<C, N>();
@@ -271,7 +281,7 @@ __global__ void __launch_bounds__(FastLB<C, N>::ROW, FastLB<C, N>::ROW_MIN) kf_i
                 C y = g[n1];
                 const C ws = cadd(wb[q], wa[q]);
                 C coef = mkc(-dc * ws.y, dc * ws.x);
-                if (CONJ) coef = cconj(coef);
+                if (conj) coef = cconj(coef);
                 const C yd = cadd(y, cmul(coef, xv[q]));
                 y = dv ? yd : y;
                 y = (!use_mask || ((fl[q] >> s) & 1)) ? y : czero<C>();
@@ -385,8 +395,9 @@ __global__ void __launch_bounds__(FastLB<C, N>::COL, FastLB<C, N>::COL_MIN) kf_i
 // then E[s][h][k1][k2][tx] (spectra) then E[s][h][k1][n2][tx] (inverse).
 // Thread roles: steps A/A' (tx, s, n2); step B / multiply / B' (tx, h, k1).
 // ---------------------------------------------------------------------------
-template <typename C, int N, bool CONJ, int TP>
-__global__ void __launch_bounds__(FastXLB<C, TP>::XT, FastXLB<C, TP>::X_MIN) kf_x_spectral(OpDev<C> op) {
+// (conj: the adjoint operator's tables and conj(Gs); a run-time flag)
+template <typename C, int N, int TP>
+__global__ void __launch_bounds__(FastXLB<C, TP>::XT, FastXLB<C, TP>::X_MIN) kf_x_spectral(OpDev<C> op, int conj) {
     if (gate_closed(op.gate)) return;
     using R = typename real_of<C>::type;
     constexpr int R1 = FastPlan<N>::R1, R2 = FastPlan<N>::R2;
@@ -429,7 +440,7 @@ __global__ void __launch_bounds__(FastXLB<C, TP>::XT, FastXLB<C, TP>::X_MIN) kf_
         const int q = threadIdx.x / TP;
         const int h = q / R1, k1 = q % R1;
         if (h < 2 && live) {
-            const int md = CONJ ? 1 : 0;
+            const int md = conj ? 1 : 0;
             C* base = E + h * HS + k1 * KS + tx;  // + s*SS + k2*TP
 #pragma unroll
             for (int s = 0; s < 3; s++) {
@@ -451,7 +462,7 @@ __global__ void __launch_bounds__(FastXLB<C, TP>::XT, FastXLB<C, TP>::X_MIN) kf_
                 const C Px = op.ax[0].P[md][sx], Qx = op.ax[0].Q[md][sx];
                 const int gx = op.ax[0].gfold[sx];
                 C G = op.Gs[((long long)gx * (op.ny + 1) + gy) * (op.nz + 1) + gz];
-                if (CONJ) G = cconj(G);
+                if (conj) G = cconj(G);
                 C* e = base + k2 * TP;
                 const C Jx = e[0], Jy = e[SS], Jz = e[2 * SS];
                 const C rho = cadd(cadd(cmul(Px, Jx), cmul(Py, Jy)), cmul(Pz, Jz));

@@ -264,6 +264,7 @@ template <int R, bool INV, typename C> __host__ __device__ __forceinline__ void 
     else if constexpr (R == 9) dft_pq<3, 3, INV>(v);
     else if constexpr (R == 10) dft_pq<2, 5, INV>(v);
     else if constexpr (R == 12) dft_pq<4, 3, INV>(v);
+    else if constexpr (R == 15) dft_pq<3, 5, INV>(v);
     else if constexpr (R == 16) dft16<INV>(v);
     else if constexpr (R % 2 == 1) dft_odd<R, INV>(v);
     else static_assert(R == 2, "unsupported register radix");

@@ -61,15 +61,10 @@ int launch_fast_z(Operator<T>& op, bool forward, Pro pro, Epi epi, const cplx_t<
         VIE_CUDA_TRY(ensure_smem(kf, smem), err);
         kf<<<grid, L * ROWS, smem, st>>>(op.dev, pro);
         count_launch();
-    } else if (conj) {
-        auto kf = kf_inv_z<C, N, true, Epi>;
-        VIE_CUDA_TRY(ensure_smem(kf, smem), err);
-        kf<<<grid, L * ROWS, smem, st>>>(op.dev, xdiag, epi, partial);
-        count_launch();
     } else {
-        auto kf = kf_inv_z<C, N, false, Epi>;
+        auto kf = kf_inv_z<C, N, Epi>;
         VIE_CUDA_TRY(ensure_smem(kf, smem), err);
-        kf<<<grid, L * ROWS, smem, st>>>(op.dev, xdiag, epi, partial);
+        kf<<<grid, L * ROWS, smem, st>>>(op.dev, xdiag, epi, partial, conj ? 1 : 0);
         count_launch();
     }
     return VIE_OK;
@@ -93,9 +88,9 @@ int launch_fast_x_tp(Operator<T>& op, bool conj, cudaStream_t st, Error& err) {
     using C = cplx_t<T>;
     constexpr size_t smem = fast_smem_x<C, N, TP>();
     dim3 grid(ceil_div(2 * op.dev.nz, TP), 2 * op.dev.ny);
-    auto kf = conj ? kf_x_spectral<C, N, true, TP> : kf_x_spectral<C, N, false, TP>;
+    auto kf = kf_x_spectral<C, N, TP>;
     VIE_CUDA_TRY(ensure_smem(kf, smem), err);
-    kf<<<grid, fast_x_threads<C, N, TP>(), smem, st>>>(op.dev);
+    kf<<<grid, fast_x_threads<C, N, TP>(), smem, st>>>(op.dev, conj ? 1 : 0);
     count_launch();
     return VIE_OK;
 }
@@ -110,7 +105,13 @@ int launch_fast_x(Operator<T>& op, bool conj, cudaStream_t st, Error& err) {
 #define VIE_FAST_SWITCH(n, CALL)                                   \
     switch (n) {                                                    \
         case 256: { constexpr int NN = 256; CALL; } break;          \
+        case 192: { constexpr int NN = 192; CALL; } break;          \
+        case 176: { constexpr int NN = 176; CALL; } break;          \
+        case 160: { constexpr int NN = 160; CALL; } break;          \
+        case 144: { constexpr int NN = 144; CALL; } break;          \
         case 128: { constexpr int NN = 128; CALL; } break;          \
+        case 120: { constexpr int NN = 120; CALL; } break;          \
+        case 112: { constexpr int NN = 112; CALL; } break;          \
         case 96: { constexpr int NN = 96; CALL; } break;            \
         case 88: { constexpr int NN = 88; CALL; } break;            \
         case 80: { constexpr int NN = 80; CALL; } break;            \
