@@ -308,25 +308,47 @@ __global__ void __launch_bounds__(kThreads) k_inv_z(OpDev<C> op, const C* __rest
     for (int k = 0; k < KA; k++) acc[k] = make_double2(0.0, 0.0);
     const long long sstep = s == 0 ? (long long)op.ny * N : (s == 1 ? (long long)N : 1LL);
     const R dc = op.dcoef[s];
-    for (int e = threadIdx.x; e < T * N; e += blockDim.x) {
-        const int t = e / N, n = e - t * N;
-        const long long row = row0 + t;
-        if (row >= nrows) continue;
-        const long long idx = row * N + n;
-        C y = czero<C>();
-        if (!(op.parts & 4) || ((op.flags[idx] >> s) & 1)) {
-            if (op.parts & 1) y = cadd(buf[n * TP + t], cmulc(buf[fs + n * TP + t], tw[n]));
+    const bool use_green = op.parts & 1, use_diag = op.parts & 2, use_mask = op.parts & 4;
+    // four elements per thread and step: all their global reads (flags, contrast
+    // pair, diagonal source, the epilogue's vector) first, then the arithmetic
+    // and stores; the selections give the branchy form's results bit for bit
+    constexpr int CH = 4;
+    const int total = T * N, stride = blockDim.x;
+    for (int e0 = threadIdx.x; e0 < total; e0 += CH * stride) {
+        long long idx[CH];
+        bool ok[CH], dv[CH];
+        unsigned char fl[CH];
+        C wa[CH], wb[CH], xv[CH], pv[CH];
+#pragma unroll
+        for (int q = 0; q < CH; q++) {
+            const int e = e0 + q * stride;
+            const int t = e / N, n = e - t * N;
+            const long long row = row0 + t;
+            ok[q] = e < total && row < nrows;
+            idx[q] = ok[q] ? row * N + n : 0;
             const int i = (int)(row / op.ny), j = (int)(row - (long long)i * op.ny);
-            const bool valid = (s != 0 || i < op.nx - 1) && (s != 1 || j < op.ny - 1) && (s != 2 || n < N - 1);
-            if ((op.parts & 2) && valid) {
-                // -i delta Z0/(2 k0) (w_a + w_b) J   (fft.h:419-433); conjugate twin :455-469
-                const C ws = cadd(op.w[idx + sstep], op.w[idx]);
-                C coef = mkc(-dc * ws.y, dc * ws.x);  // i * dc * ws with dc = -delta Z0/(2 k0)
-                if (CONJ) coef = cconj(coef);
-                y = cadd(y, cmul(coef, xin[(long long)s * op.a + idx]));
-            }
+            dv[q] = ok[q] && (s != 0 || i < op.nx - 1) && (s != 1 || j < op.ny - 1) && (s != 2 || n < N - 1);
+            fl[q] = op.flags[idx[q]];
+            wa[q] = op.w[idx[q]];
+            wb[q] = op.w[dv[q] ? idx[q] + sstep : idx[q]];
+            xv[q] = xin[(long long)s * op.a + idx[q]];
+            pv[q] = epi.pre(s, idx[q]);
         }
-        epi(s, idx, y, acc);
+#pragma unroll
+        for (int q = 0; q < CH; q++) {
+            if (!ok[q]) continue;
+            const int e = e0 + q * stride;
+            const int t = e / N, n = e - t * N;
+            C y = use_green ? cadd(buf[n * TP + t], cmulc(buf[fs + n * TP + t], tw[n])) : czero<C>();
+            // -i delta Z0/(2 k0) (w_a + w_b) J   (fft.h:419-433); conjugate twin :455-469
+            const C ws = cadd(wb[q], wa[q]);
+            C coef = mkc(-dc * ws.y, dc * ws.x);  // i * dc * ws with dc = -delta Z0/(2 k0)
+            if (CONJ) coef = cconj(coef);
+            const C yd = cadd(y, cmul(coef, xv[q]));
+            y = (use_diag && dv[q]) ? yd : y;
+            y = (!use_mask || ((fl[q] >> s) & 1)) ? y : czero<C>();
+            epi.put(s, idx[q], y, acc, pv[q]);
+        }
     }
     if constexpr (Epi::K > 0) block_reduce_store<KA>(acc, partial, (long long)blockIdx.y * gridDim.x + blockIdx.x);
 }
