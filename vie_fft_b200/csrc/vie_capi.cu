@@ -52,6 +52,8 @@ TileCfg tiles_from_env() {
     }
     // VIE_XTILE=1: the register x pass with the half pencil tile (otherwise the autotuner decides)
     if (const char* x = std::getenv("VIE_XTILE")) t.xalt = std::atoi(x) == 1 ? 1 : 0;
+    // VIE_TMA=0: the y passes with plain loads instead of TMA-staged tiles
+    if (const char* x = std::getenv("VIE_TMA")) t.ytma = std::atoi(x) == 0 ? 0 : 1;
     return t;
 }
 
@@ -345,7 +347,7 @@ int vie_apply(vie_ctx* ctx, const double* x, double* y, int conj, int parts) {
     if (e != cudaSuccess) rc = ctx->set_error(VIE_ERR_CUDA, cudaGetErrorString(e));
     cudaFree(dx);
     cudaFree(dy);
-    return rc;
+    return ctx->check_waits(rc);
 }
 
 int vie_reset(vie_ctx* ctx, double* v, int comp) {
@@ -383,7 +385,7 @@ int vie_solve(vie_ctx* ctx, const vie_solve_params* p, double* x, vie_solve_info
         if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
         if (e != cudaSuccess && !rc) rc = ctx->set_error(VIE_ERR_CUDA, cudaGetErrorString(e));
     }
-    return rc;
+    return ctx->check_waits(rc);
 }
 
 int vie_solve_batch(vie_ctx* const* ctxs, int n, const vie_solve_params* p, vie_solve_info* infos) {
@@ -402,7 +404,13 @@ int vie_solve_batch(vie_ctx* const* ctxs, int n, const vie_solve_params* p, vie_
     }
     if (!(p->tol > 0)) return ctxs[0]->set_error(VIE_ERR_ARG, "tolerance must be positive");
     cudaSetDevice(ctxs[0]->device);
-    return solve_batch_driver(ctxs, n, p, infos);
+    int rc = solve_batch_driver(ctxs, n, p, infos);
+    cudaStreamSynchronize(ctxs[0]->stream);
+    for (int i = 0; i < n; i++) {
+        const int w = ctxs[i]->check_waits(VIE_OK);
+        if (w && !rc) rc = w;
+    }
+    return rc;
 }
 
 int vie_power_grad(vie_ctx* ctx, const unsigned char* edge_mask, const vie_solve_params* p, double* power,
@@ -418,6 +426,7 @@ int vie_power_grad(vie_ctx* ctx, const unsigned char* edge_mask, const vie_solve
     ctx->err.code = VIE_OK;
     ctx->err.msg.clear();
     rc = power_grad_driver(ctx, edge_mask, p, power, grad, info_fwd, info_adj);
+    rc = ctx->check_waits(rc);
     if (!rc) ctx->have_x = true;
     return rc;
 }
@@ -512,7 +521,7 @@ int vie_stream(vie_ctx* ctx, void** stream) {
 int vie_sync(vie_ctx* ctx) {
     if (check_ctx(ctx)) return VIE_ERR_ARG;
     CTX_CUDA(cudaStreamSynchronize(ctx->stream));
-    return VIE_OK;
+    return ctx->check_waits(VIE_OK);
 }
 
 }  // extern "C"

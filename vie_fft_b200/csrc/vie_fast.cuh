@@ -18,6 +18,8 @@
 //   column passes (pencils contiguous in memory): tid = lane * TP + tx,
 //   row passes (pencils are contiguous rows):     tid = row * L + lane.
 #pragma once
+#include <cuda.h>
+
 #include "vie_operator.cuh"
 
 namespace vie {
@@ -341,6 +343,108 @@ __global__ void __launch_bounds__(FastLB<C, N>::COL, FastLB<C, N>::COL_MIN) kf_f
     }
 }
 
+// F2 with its pencil tile staged by TMA: one cp.async.bulk.tensor load of the
+// [N rows x TP columns] slab tile into the front of E (the shared buffer the
+// pass transposes through), completion on an mbarrier, then the same
+// arithmetic as kf_fwd_y reading its inputs from shared memory.  The tensor
+// map views b as 2D (columns: 2 Lz reals, rows: 3 nx N).  The x coordinate,
+// 2 kz0 reals = 8 kz0 (FP32) or 16 kz0 (FP64) bytes with kz0 a multiple of TP,
+// is always a multiple of 128 bytes; no multicast.  The wait is bounded: if
+// the copy has not completed after kTmaWaitIters polls the CTA records the
+// failure in op.status (read back by the host) and returns.
+constexpr int kTmaWaitIters = 1 << 22;
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned bar, unsigned phase) {
+    for (int it = 0; it < kTmaWaitIters; it++) {
+        unsigned ok;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(ok)
+            : "r"(bar), "r"(phase)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
+template <typename C, int N>
+__global__ void __launch_bounds__(FastLB<C, N>::COL, FastLB<C, N>::COL_MIN)
+    kf_fwd_y_tma(OpDev<C> op, const __grid_constant__ CUtensorMap tm) {
+    if (gate_closed(op.gate)) return;
+    constexpr int R1 = FastPlan<N>::R1, R2 = FastPlan<N>::R2, TP = FastTiles<C>::TP_Y;
+    constexpr int HS = N * TP;
+    __shared__ __align__(8) unsigned long long bar;
+    C* tw;
+    C* E = fast_smem<C, N>(op.ax[1].tw, tw);
+    // the TMA destination 128-byte aligned (the launch reserves 128 more bytes)
+    E = reinterpret_cast<C*>(reinterpret_cast<char*>(E) + ((128u - (smem_u32(E) & 127u)) & 127u));
+    const int tx = threadIdx.x % TP, lane = threadIdx.x / TP;
+    const int Lz = 2 * op.nz;
+    const int kz = blockIdx.x * TP + tx, i = blockIdx.y, s = blockIdx.z;
+    const bool live = kz < Lz;
+    const unsigned b = smem_u32(&bar);
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned bytes = (unsigned)(sizeof(C) * N * TP);
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(bytes) : "memory");
+        const int x = 2 * (int)blockIdx.x * TP;                    // reals
+        const int y = ((int)blockIdx.z * op.nx + (int)blockIdx.y) * N;  // rows
+        asm volatile(
+            "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+            ::"r"(smem_u32(E)), "l"(&tm), "r"(x), "r"(y), "r"(b)
+            : "memory");
+    }
+    // the whole block takes the same branch: a wait that ran out in any thread
+    // sets the status word, waits once more (bounded) for the copy in flight and
+    // leaves the pass undone
+    if (__syncthreads_or(!mbar_wait_bounded(b, 0))) {
+        if (threadIdx.x == 0 && op.status) *(volatile int*)op.status = 1;
+        mbar_wait_bounded(b, 0);
+        return;
+    }
+    // inputs of this thread from the staged tile (row n = n2 + R2 n1, column tx)
+    C v[R1];
+    const int n2 = lane;
+    if (lane < R2 && live) {
+#pragma unroll
+        for (int n1 = 0; n1 < R1; n1++) v[n1] = E[(n2 + R2 * n1) * TP + tx];
+    }
+    __syncthreads();  // the tile is overwritten below
+    if (lane < R2 && live) {
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            C a[R1];
+#pragma unroll
+            for (int n1 = 0; n1 < R1; n1++) a[n1] = h ? cmul(v[n1], tw[n2 + R2 * n1]) : v[n1];
+            dft_reg<R1, false>(a);
+#pragma unroll
+            for (int k1 = 0; k1 < R1; k1++)
+                E[h * HS + (k1 * R2 + n2) * TP + tx] = k1 ? cmul(a[k1], tw[2 * n2 * k1]) : a[k1];
+        }
+    }
+    __syncthreads();
+    if (lane < R1 && live) {
+        const int k1 = lane;
+        C* dst = op.c + ((long long)s * op.nx + i) * (long long)(2 * N) * Lz;
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            C X[R2];
+#pragma unroll
+            for (int n2b = 0; n2b < R2; n2b++) X[n2b] = E[h * HS + (k1 * R2 + n2b) * TP + tx];
+            dft_reg<R2, false>(X);
+#pragma unroll
+            for (int k2 = 0; k2 < R2; k2++) dst[(long long)(h * N + k1 + R1 * k2) * Lz + kz] = X[k2];
+        }
+    }
+}
+
 // I2 (column pass): inverse y, crop.  E layout: E[h][n2][k1][tx].
 template <typename C, int N>
 __global__ void __launch_bounds__(FastLB<C, N>::COL, FastLB<C, N>::COL_MIN) kf_inv_y(OpDev<C> op) {
@@ -376,6 +480,88 @@ __global__ void __launch_bounds__(FastLB<C, N>::COL, FastLB<C, N>::COL_MIN) kf_i
         for (int k1 = 0; k1 < R1; k1++) {
             y0[k1] = E[(n2 * R1 + k1) * TP + tx];
             y1[k1] = E[HS + (n2 * R1 + k1) * TP + tx];
+        }
+        dft_reg<R1, true>(y0);
+        dft_reg<R1, true>(y1);
+        C* dst = op.b + ((long long)s * op.nx + i) * (long long)N * Lz;
+#pragma unroll
+        for (int n1 = 0; n1 < R1; n1++) {
+            const int n = n2 + R2 * n1;
+            dst[(long long)n * Lz + kz] = cadd(y0[n1], cmulc(y1[n1], tw[n]));
+        }
+    }
+}
+
+// I2 with its tile staged by TMA: the [2N rows x TP columns] spectra tile as two
+// boxes of N rows (the box height limit is 256) into E, one mbarrier; the same
+// alignment, bounded wait and arithmetic rules as kf_fwd_y_tma.  Each half is
+// read into registers before its results overwrite its part of E.
+template <typename C, int N>
+__global__ void __launch_bounds__(FastLB<C, N>::COL, FastLB<C, N>::COL_MIN)
+    kf_inv_y_tma(OpDev<C> op, const __grid_constant__ CUtensorMap tm) {
+    if (gate_closed(op.gate)) return;
+    constexpr int R1 = FastPlan<N>::R1, R2 = FastPlan<N>::R2, TP = FastTiles<C>::TP_Y;
+    constexpr int HS = N * TP;
+    __shared__ __align__(8) unsigned long long bar;
+    C* tw;
+    C* E = fast_smem<C, N>(op.ax[1].tw, tw);
+    E = reinterpret_cast<C*>(reinterpret_cast<char*>(E) + ((128u - (smem_u32(E) & 127u)) & 127u));
+    const int tx = threadIdx.x % TP, lane = threadIdx.x / TP;
+    const int Lz = 2 * op.nz;
+    const int kz = blockIdx.x * TP + tx, i = blockIdx.y, s = blockIdx.z;
+    const bool live = kz < Lz;
+    const unsigned b = smem_u32(&bar);
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned bytes = (unsigned)(sizeof(C) * 2 * N * TP);
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(bytes) : "memory");
+        const int x = 2 * (int)blockIdx.x * TP;
+        const int y = ((int)blockIdx.z * op.nx + (int)blockIdx.y) * 2 * N;
+#pragma unroll
+        for (int h = 0; h < 2; h++)
+            asm volatile(
+                "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+                "[%4];" ::"r"(smem_u32(E + h * HS)),
+                "l"(&tm), "r"(x), "r"(y + h * N), "r"(b)
+                : "memory");
+    }
+    // the whole block takes the same branch: a wait that ran out in any thread
+    // sets the status word, waits once more (bounded) for the copy in flight and
+    // leaves the pass undone
+    if (__syncthreads_or(!mbar_wait_bounded(b, 0))) {
+        if (threadIdx.x == 0 && op.status) *(volatile int*)op.status = 1;
+        mbar_wait_bounded(b, 0);
+        return;
+    }
+    const int k1 = lane;
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        C X[R2];
+        if (lane < R1 && live) {
+#pragma unroll
+            for (int k2 = 0; k2 < R2; k2++) X[k2] = E[h * HS + (k1 + R1 * k2) * TP + tx];
+        }
+        __syncthreads();  // this half of the tile is overwritten below
+        if (lane < R1 && live) {
+            dft_reg<R2, true>(X);
+#pragma unroll
+            for (int n2 = 0; n2 < R2; n2++)
+                E[h * HS + (n2 * R1 + k1) * TP + tx] = n2 ? cmulc(X[n2], tw[2 * n2 * k1]) : X[n2];
+        }
+    }
+    __syncthreads();
+    if (lane < R2 && live) {
+        const int n2 = lane;
+        C y0[R1], y1[R1];
+#pragma unroll
+        for (int q = 0; q < R1; q++) {
+            y0[q] = E[(n2 * R1 + q) * TP + tx];
+            y1[q] = E[HS + (n2 * R1 + q) * TP + tx];
         }
         dft_reg<R1, true>(y0);
         dft_reg<R1, true>(y1);

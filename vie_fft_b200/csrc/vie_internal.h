@@ -1,5 +1,6 @@
 // vie_internal.h -- host-side structures of the VIE library (not part of the ABI).
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <atomic>
@@ -47,6 +48,7 @@ struct TileCfg {
     int tz = 0, tc = 0, tx = 0;
     int fast[3] = {-1, -1, -1};  // per axis: 1 register four-step kernels, 0 generic, -1 automatic
     int xalt = 0;                // register x pass with the half pencil tile
+    int ytma = 1;                // register y passes with their tiles staged by TMA (0: plain loads)
 };
 
 // Operator state for one arithmetic precision.  Owns its tables, the Green
@@ -63,6 +65,19 @@ template <typename T> struct Operator {
     C* d_b = nullptr;
     C* d_c = nullptr;
     bool owns_scratch = true;
+    // TMA view of the b scratch for the forward y pass (2D: 2 Lz reals x 3 nx ny rows)
+    CUtensorMap tm_b{};
+    bool tm_b_ok = false;
+    bool use_ytma = false;
+    const void* tm_b_addr = nullptr;  // the buffer tm_b was encoded for
+    CUtensorMap tm_c{};          // TMA view of the c spectra for the inverse y pass
+    bool tm_c_ok = false;
+    const void* tm_c_addr = nullptr;
+    // set to 1 by a kernel whose bounded wait ran out: one word of mapped pinned
+    // host memory (h_status), so the host reads it after a synchronisation
+    // without a copy
+    int* h_status = nullptr;
+    int* d_status = nullptr;
 
     int init(int nx, int ny, int nz, const double d[3], double k0, const TileCfg& tiles,
              const AxisPlan plans[3], const unsigned char* d_flags, Error& err);
@@ -74,6 +89,12 @@ template <typename T> struct Operator {
     // y = A x (conj: A^H), plain store
     int apply(const C* x, C* y, bool conj, cudaStream_t st, Error& err);
     size_t scratch_bytes() const;
+    // true (and the word cleared) when a bounded device wait ran out since the last call
+    bool take_timeout() {
+        if (!h_status || !*(volatile int*)h_status) return false;
+        *(volatile int*)h_status = 0;
+        return true;
+    }
 };
 
 // Device-resident Krylov scalars (FP64 complex), one block per solve.
@@ -159,5 +180,12 @@ struct vie_ctx {
         err.code = code;
         err.msg = m;
         return code;
+    }
+    // after a synchronisation: VIE_ERR_TIMEOUT when a kernel's bounded wait on
+    // its staged tile ran out since the last check (its pass was left undone)
+    int check_waits(int rc) {
+        const bool t64 = op64.take_timeout(), t32 = op32.take_timeout();
+        if (t64 || t32) return set_error(VIE_ERR_TIMEOUT, "a TMA tile load did not complete within its bounded wait");
+        return rc;
     }
 };

@@ -76,6 +76,15 @@ int launch_fast_y(Operator<T>& op, bool forward, cudaStream_t st, Error& err) {
     constexpr int TP = FastTiles<C>::TP_Y, L = fast_lanes<C, N>();
     constexpr size_t smem = fast_smem_col<C, N>();
     dim3 grid(ceil_div(2 * op.dev.nz, TP), op.dev.nx, 3);
+    if (op.use_ytma && op.dev.b == op.tm_b_addr && op.dev.c == op.tm_c_addr) {
+        // tiles staged by TMA (default; the autotuner may switch it off); 128 more
+        // bytes of shared memory to align the destination
+        auto kt = forward ? kf_fwd_y_tma<C, N> : kf_inv_y_tma<C, N>;
+        VIE_CUDA_TRY(ensure_smem(kt, smem + 128), err);
+        kt<<<grid, TP * L, smem + 128, st>>>(op.dev, forward ? op.tm_b : op.tm_c);
+        count_launch();
+        return VIE_OK;
+    }
     auto kf = forward ? kf_fwd_y<C, N> : kf_inv_y<C, N>;
     VIE_CUDA_TRY(ensure_smem(kf, smem), err);
     kf<<<grid, TP * L, smem, st>>>(op.dev);

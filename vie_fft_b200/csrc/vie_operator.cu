@@ -51,6 +51,24 @@ std::vector<int> axis_perm(const AxisPlan& pl) {
     return perm;
 }
 
+// cuTensorMapEncodeTiled from the driver, through the runtime (no link to libcuda)
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static EncodeTiledFn encode_tiled() {
+    static EncodeTiledFn fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    }
+    return fn;
+}
+
 template <typename C> static C to_c(double re, double im);
 template <> float2 to_c<float2>(double re, double im) { return make_float2((float)re, (float)im); }
 template <> double2 to_c<double2>(double re, double im) { return make_double2(re, im); }
@@ -185,6 +203,39 @@ int Operator<T>::init(int nx, int ny, int nz, const double d[3], double k0, cons
     o.flags = d_flags;
     o.b = d_b;
     o.c = d_c;
+    // status word of the bounded waits, and the TMA view of b for the forward y pass
+    if (!h_status) {
+        VIE_CUDA_TRY(cudaHostAlloc(&h_status, sizeof(int), cudaHostAllocMapped), err);
+        *h_status = 0;
+        VIE_CUDA_TRY(cudaHostGetDevicePointer(&d_status, h_status, 0), err);
+    }
+    o.status = d_status;
+    use_ytma = tm_b_ok = tm_c_ok = false;
+    tm_b_addr = tm_c_addr = nullptr;
+    if (o.fast[1] && tiles.ytma && d_b && d_c && ny <= 256) {
+        if (EncodeTiledFn enc = encode_tiled()) {
+            constexpr int TPY = FastTiles<C>::TP_Y;
+            const cuuint64_t dims[2] = {(cuuint64_t)4 * nz, (cuuint64_t)3 * nx * ny};  // reals, rows
+            const cuuint64_t strides[1] = {(cuuint64_t)4 * nz * sizeof(T)};             // bytes per row
+            const cuuint32_t box[2] = {(cuuint32_t)2 * TPY, (cuuint32_t)ny};
+            const cuuint32_t estr[2] = {1, 1};
+            const CUresult r = enc(&tm_b, sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                                   2, d_b, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                   CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+            tm_b_ok = r == CUDA_SUCCESS;
+            tm_b_addr = d_b;
+            // c: 2 Lz reals x 3 nx 2ny rows, boxes of ny rows (one half of a y line)
+            const cuuint64_t dims_c[2] = {(cuuint64_t)4 * nz, (cuuint64_t)6 * nx * ny};
+            const CUresult rc2 = enc(&tm_c, sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                                     2, d_c, dims_c, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                     CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+            tm_c_ok = rc2 == CUDA_SUCCESS;
+            tm_c_addr = d_c;
+            use_ytma = tm_b_ok && tm_c_ok;
+        }
+    }
     ready = true;
     return VIE_OK;
 }
@@ -232,7 +283,11 @@ template <typename T> void Operator<T>::release() {
         if (d_b) cudaFree(d_b);
         if (d_c) cudaFree(d_c);
     }
+    if (h_status) cudaFreeHost(h_status);
     d_tables = nullptr; d_Gs = nullptr; d_w = nullptr; d_b = nullptr; d_c = nullptr;
+    h_status = d_status = nullptr;
+    dev.status = nullptr;
+    use_ytma = tm_b_ok = tm_c_ok = false;
     ready = false;
 }
 

@@ -68,6 +68,7 @@ template <typename C> struct OpDev {
     C* b;                      // 3 * nx*ny*2nz scratch
     C* c;                      // 3 * nx*2ny*2nz scratch
     Gate gate;                 // launch gate of the current solve (state == nullptr: always run)
+    int* status;               // device word set by a kernel whose bounded wait ran out (TMA staging)
 };
 
 __host__ __device__ inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }

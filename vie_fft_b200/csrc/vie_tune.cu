@@ -50,7 +50,8 @@ std::string plan_str(const AxisPlan& p) {
     return s;
 }
 
-// one line per entry: key(5 ints) then per axis: fast tile nst radices..., then ms
+// one line per entry: key(5 ints) then per axis: fast tile nst radices..., then
+// xalt, ms and ytma (absent in older files: TMA staging on)
 std::string serialize(const std::string& key, const Sched& s) {
     std::ostringstream o;
     o << key;
@@ -59,7 +60,7 @@ std::string serialize(const std::string& key, const Sched& s) {
         o << ' ' << s.t.fast[ax] << ' ' << tile[ax] << ' ' << s.plan[ax].nst;
         for (int i = 0; i < s.plan[ax].nst; i++) o << ' ' << s.plan[ax].rad[i];
     }
-    o << ' ' << s.t.xalt << ' ' << s.ms;
+    o << ' ' << s.t.xalt << ' ' << s.ms << ' ' << s.t.ytma;
     return o.str();
 }
 
@@ -92,6 +93,8 @@ void load_file_locked() {
         }
         ok = ok && (in >> s.t.xalt >> s.ms) && (s.t.xalt == 0 || s.t.xalt == 1);
         if (!ok) continue;
+        int ytma = 1;
+        if (in >> ytma) s.t.ytma = ytma == 0 ? 0 : 1;
         s.t.tx = tile[0];
         s.t.tc = tile[1];
         s.t.tz = tile[2];
@@ -191,6 +194,10 @@ template <typename T> int tune_one(vie_ctx* ctx, Operator<T>& op, Sched& best, s
                 s.t.xalt = 1;
                 cands.push_back(s);
             }
+            if (ax == 1) {  // the register y passes with TMA staging switched the other way
+                s.t.ytma = 1 - s.t.ytma;
+                cands.push_back(s);
+            }
         }
         Sched bestg;
         float bestg_ms = 1e30f;
@@ -239,7 +246,7 @@ template <typename T> int tune_one(vie_ctx* ctx, Operator<T>& op, Sched& best, s
         for (int ax = 0; ax < 3; ax++) {
             o << ' ' << nm[ax] << '=';
             if (best.t.fast[ax] == 1 || (best.t.fast[ax] < 0 && fast_length(n[ax])))
-                o << "fast" << (ax == 0 && best.t.xalt ? "/half-tile" : "");
+                o << "fast" << (ax == 0 && best.t.xalt ? "/half-tile" : "") << (ax == 1 && best.t.ytma ? "/tma" : "");
             else o << "generic[" << plan_str(best.plan[ax]) << "]/t" << tl[ax];
         }
         report = o.str();
