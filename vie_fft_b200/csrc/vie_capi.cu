@@ -54,6 +54,8 @@ TileCfg tiles_from_env() {
     if (const char* x = std::getenv("VIE_XTILE")) t.xalt = std::atoi(x) == 1 ? 1 : 0;
     // VIE_TMA=0: the y passes with plain loads instead of TMA-staged tiles
     if (const char* x = std::getenv("VIE_TMA")) t.ytma = std::atoi(x) == 0 ? 0 : 1;
+    // VIE_ZSTAGE=0: the z passes with element loads instead of rows staged by bulk copies
+    if (const char* x = std::getenv("VIE_ZSTAGE")) t.zstage = std::atoi(x) == 0 ? 0 : 1;
     return t;
 }
 

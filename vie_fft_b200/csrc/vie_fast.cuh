@@ -19,6 +19,7 @@
 //   row passes (pencils are contiguous rows):     tid = row * L + lane.
 #pragma once
 #include <cuda.h>
+#include <type_traits>
 
 #include "vie_operator.cuh"
 
@@ -118,6 +119,61 @@ template <typename C, int TP> struct FastXLB {
 };
 
 // ---------------------------------------------------------------------------
+// Asynchronous staging into shared memory (TMA unit).  Every wait on an
+// mbarrier is bounded: after kTmaWaitIters polls the block records the failure
+// in op.status (mapped host memory, read by the host after the call), waits
+// once more (bounded) for the copy still in flight and leaves its tile undone.
+constexpr int kTmaWaitIters = 1 << 22;
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned bar, unsigned phase) {
+    for (int it = 0; it < kTmaWaitIters; it++) {
+        unsigned ok;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(ok)
+            : "r"(bar), "r"(phase)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void mbar_init_one(unsigned bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect(unsigned bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+// contiguous global -> shared copy; both addresses 16-byte aligned, bytes a multiple of 16
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, unsigned bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+__device__ __forceinline__ bool aligned16(const void* p) { return ((unsigned long long)p & 15ull) == 0; }
+// two consecutive complex values (16-byte aligned pair address for float2)
+template <typename C> __device__ __forceinline__ void st_pair(C* p, C a, C b) {
+    p[0] = a;
+    p[1] = b;
+}
+template <> __device__ __forceinline__ void st_pair<float2>(float2* p, float2 a, float2 b) {
+    *reinterpret_cast<float4*>(p) = make_float4(a.x, a.y, b.x, b.y);
+}
+
+// Prologues whose source vectors the forward z pass stages whole rows of:
+// Pro::NSTAGE vectors (layout s a + idx) returned by stage_src(k), and
+// load_staged() building the prologue's operands from the staged values (any
+// other operand it still reads from global memory).  Prologues without
+// NSTAGE read everything element by element.
+template <class P, class = void> struct stage_count { static constexpr int value = 0; };
+template <class P> struct stage_count<P, std::void_t<decltype(P::NSTAGE)>> { static constexpr int value = P::NSTAGE; };
+
+// ---------------------------------------------------------------------------
 // F1 (row pass): forward z with padding fused into the load.
 // E layout: E[h][row][k1][n2], k1 stride R2 + 1 (conflict-free transposed reads).
 // ---------------------------------------------------------------------------
@@ -134,19 +190,62 @@ __global__ void __launch_bounds__(FastLB<C, N>::ROW, FastLB<C, N>::ROW_MIN) kf_f
     const long long nrows = (long long)op.nx * op.ny;
     const long long row = (long long)blockIdx.x * ROWS + r;
     const bool live = row < nrows;
+    // the prologue's source rows of this block staged whole into E (when they fit
+    // and are 16-byte aligned), then read from shared memory
+    constexpr int NS = stage_count<Pro>::value;
+    constexpr int ESZ = 2 * (R1 * (R2 + 1) > R2 * (R1 + 1) ? R1 * (R2 + 1) : R2 * (R1 + 1)) * ROWS;
+    constexpr bool kCanStage = NS > 0 && NS * ROWS * N <= ESZ;
+    __shared__ __align__(8) unsigned long long zbar;
+    bool staged = false;
+    const long long row0 = (long long)blockIdx.x * ROWS;
+    const int nr = (int)(nrows - row0 < ROWS ? nrows - row0 : ROWS);
+    if constexpr (kCanStage) {
+        staged = op.zstage != 0;
+#pragma unroll
+        for (int k = 0; k < NS; k++) staged = staged && aligned16(pro.stage_src(k) + s * op.a + row0 * N);
+        if (staged && threadIdx.x == 0) mbar_init_one(smem_u32(&zbar));
+    }
     __syncthreads();
+    if constexpr (kCanStage) {
+        if (staged) {
+            const unsigned b = smem_u32(&zbar);
+            if (threadIdx.x == 0) {
+                const unsigned bytes = (unsigned)(sizeof(C) * N) * (unsigned)nr;
+                mbar_expect(b, bytes * NS);
+#pragma unroll
+                for (int k = 0; k < NS; k++) bulk_load(E + k * ROWS * N, pro.stage_src(k) + s * op.a + row0 * N, bytes, b);
+            }
+            if (__syncthreads_or(!mbar_wait_bounded(b, 0))) {
+                if (threadIdx.x == 0 && op.status) *(volatile int*)op.status = 1;
+                mbar_wait_bounded(b, 0);
+                return;
+            }
+        }
+    }
+    C v[R1];
     if (lane < R2 && live) {
         const int n2 = lane;
         const int i = (int)(row / op.ny), j = (int)(row - (long long)i * op.ny);
         const bool vrow = (s != 0 || i < op.nx - 1) && (s != 1 || j < op.ny - 1);
-        C v[R1];
         // the prologue's reads of a chunk of elements first, then its arithmetic and stores
         constexpr int CH = R1 % 4 == 0 ? 4 : 1;
 #pragma unroll
         for (int c0 = 0; c0 < R1; c0 += CH) {
             typename Pro::L ld[CH];
 #pragma unroll
-            for (int q = 0; q < CH; q++) ld[q] = pro.load(s, row * N + n2 + R2 * (c0 + q));
+            for (int q = 0; q < CH; q++) {
+                const int n = n2 + R2 * (c0 + q);
+                if constexpr (kCanStage) {
+                    if (staged) {
+                        C sv[NS > 0 ? NS : 1];
+#pragma unroll
+                        for (int k = 0; k < NS; k++) sv[k] = E[k * ROWS * N + r * N + n];
+                        ld[q] = pro.load_staged(s, row * N + n, sv);
+                        continue;
+                    }
+                }
+                ld[q] = pro.load(s, row * N + n);
+            }
 #pragma unroll
             for (int q = 0; q < CH; q++) {
                 const int n = n2 + R2 * (c0 + q);
@@ -155,6 +254,12 @@ __global__ void __launch_bounds__(FastLB<C, N>::ROW, FastLB<C, N>::ROW_MIN) kf_f
                 v[c0 + q] = valid ? x : czero<C>();
             }
         }
+    }
+    if constexpr (kCanStage) {
+        if (staged) __syncthreads();  // the staged rows are overwritten below
+    }
+    if (lane < R2 && live) {
+        const int n2 = lane;
 #pragma unroll
         for (int h = 0; h < 2; h++) {
             C a[R1];
@@ -169,15 +274,43 @@ __global__ void __launch_bounds__(FastLB<C, N>::ROW, FastLB<C, N>::ROW_MIN) kf_f
         }
     }
     __syncthreads();
+    C X[2][R2];
     if (lane < R1 && live) {
         const int k1 = lane;
-        C X[2][R2];
 #pragma unroll
         for (int h = 0; h < 2; h++) {
 #pragma unroll
             for (int n2 = 0; n2 < R2; n2++) X[h][n2] = E[h * HS + (r * R1 + k1) * SR + n2];
             dft_reg<R2, false>(X[h]);
         }
+    }
+    // the block's output rows are contiguous: gathered in E in their global
+    // order and written by one bulk copy (when 16-byte aligned)
+    C* bdst = op.b + ((long long)s * nrows + row0) * (2 * N);
+    if (op.zstage && aligned16(bdst)) {
+        __syncthreads();  // every read of E is done
+        if (lane < R1 && live) {
+            const int k1 = lane;
+#pragma unroll
+            for (int k2 = 0; k2 < R2; k2++) {
+                const int m = k1 + R1 * k2;
+                st_pair(E + r * (2 * N) + 2 * m, X[0][k2], X[1][k2]);
+            }
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const unsigned bytes = (unsigned)(sizeof(C) * 2 * N) * (unsigned)nr;
+            asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(bdst), "r"(smem_u32(E)),
+                         "r"(bytes)
+                         : "memory");
+            asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+            asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+        }
+        return;
+    }
+    if (lane < R1 && live) {
+        const int k1 = lane;
         C* dst = op.b + ((long long)s * nrows + row) * (2 * N);
 #pragma unroll
         for (int k2 = 0; k2 < R2; k2++) {
@@ -209,17 +342,51 @@ __global__ void __launch_bounds__(FastLB<C, N>::ROW, FastLB<C, N>::ROW_MIN) kf_i
     const long long nrows = (long long)op.nx * op.ny;
     const long long row = (long long)blockIdx.x * ROWS + r;
     const bool live = row < nrows;
+    // the block's spectra rows (contiguous) staged whole into E by one bulk copy
+    __shared__ __align__(8) unsigned long long zbar;
+    const long long row0 = (long long)blockIdx.x * ROWS;
+    const int nr = (int)(nrows - row0 < ROWS ? nrows - row0 : ROWS);
+    const C* bsrc = op.b + ((long long)s * nrows + row0) * (2 * N);
+    const bool staged = op.zstage != 0 && aligned16(bsrc);
+    if (staged && threadIdx.x == 0) mbar_init_one(smem_u32(&zbar));
     __syncthreads();
+    if (staged) {
+        const unsigned b = smem_u32(&zbar);
+        if (threadIdx.x == 0) {
+            const unsigned bytes = (unsigned)(sizeof(C) * 2 * N) * (unsigned)nr;
+            mbar_expect(b, bytes);
+            bulk_load(E, bsrc, bytes, b);
+        }
+        if (__syncthreads_or(!mbar_wait_bounded(b, 0))) {
+            if (threadIdx.x == 0 && op.status) *(volatile int*)op.status = 1;
+            mbar_wait_bounded(b, 0);
+            return;
+        }
+    }
+    C X[2][R2];
     if (lane < R1 && live) {
         const int k1 = lane;
-        const C* src = op.b + ((long long)s * nrows + row) * (2 * N);
-        C X[2][R2];
+        if (staged) {
+            const C* src = E + r * (2 * N);
 #pragma unroll
-        for (int k2 = 0; k2 < R2; k2++) {
-            const int m = k1 + R1 * k2;
-            X[0][k2] = src[2 * m];
-            X[1][k2] = src[2 * m + 1];
+            for (int k2 = 0; k2 < R2; k2++) {
+                const int m = k1 + R1 * k2;
+                X[0][k2] = src[2 * m];
+                X[1][k2] = src[2 * m + 1];
+            }
+        } else {
+            const C* src = op.b + ((long long)s * nrows + row) * (2 * N);
+#pragma unroll
+            for (int k2 = 0; k2 < R2; k2++) {
+                const int m = k1 + R1 * k2;
+                X[0][k2] = src[2 * m];
+                X[1][k2] = src[2 * m + 1];
+            }
         }
+    }
+    if (staged) __syncthreads();  // the staged rows are overwritten below
+    if (lane < R1 && live) {
+        const int k1 = lane;
 #pragma unroll
         for (int h = 0; h < 2; h++) {
             dft_reg<R2, true>(X[h]);
@@ -349,25 +516,8 @@ __global__ void __launch_bounds__(FastLB<C, N>::COL, FastLB<C, N>::COL_MIN) kf_f
 // arithmetic as kf_fwd_y reading its inputs from shared memory.  The tensor
 // map views b as 2D (columns: 2 Lz reals, rows: 3 nx N).  The x coordinate,
 // 2 kz0 reals = 8 kz0 (FP32) or 16 kz0 (FP64) bytes with kz0 a multiple of TP,
-// is always a multiple of 128 bytes; no multicast.  The wait is bounded: if
-// the copy has not completed after kTmaWaitIters polls the CTA records the
-// failure in op.status (read back by the host) and returns.
-constexpr int kTmaWaitIters = 1 << 22;
-
-__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ bool mbar_wait_bounded(unsigned bar, unsigned phase) {
-    for (int it = 0; it < kTmaWaitIters; it++) {
-        unsigned ok;
-        asm volatile(
-            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-            : "=r"(ok)
-            : "r"(bar), "r"(phase)
-            : "memory");
-        if (ok) return true;
-    }
-    return false;
-}
+// is always a multiple of 128 bytes; no multicast.  The wait is bounded (see
+// mbar_wait_bounded).
 
 template <typename C, int N>
 __global__ void __launch_bounds__(FastLB<C, N>::COL, FastLB<C, N>::COL_MIN)
@@ -646,7 +796,9 @@ __global__ void __launch_bounds__(FastXLB<C, TP>::XT, FastXLB<C, TP>::X_MIN) kf_
             for (int k2 = 0; k2 < R2; k2++) {
                 const int sx = h * N + k1 + R1 * k2;
                 const C Px = op.ax[0].P[md][sx], Qx = op.ax[0].Q[md][sx];
-                const int gx = op.ax[0].gfold[sx];
+                // slot h N + m holds frequency k = 2m + h; its octant index folds k > N
+                const int kx = 2 * (k1 + R1 * k2) + h;
+                const int gx = kx <= N ? kx : 2 * N - kx;
                 C G = op.Gs[((long long)gx * (op.ny + 1) + gy) * (op.nz + 1) + gz];
                 if (conj) G = cconj(G);
                 C* e = base + k2 * TP;

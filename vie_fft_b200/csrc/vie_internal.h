@@ -49,6 +49,7 @@ struct TileCfg {
     int fast[3] = {-1, -1, -1};  // per axis: 1 register four-step kernels, 0 generic, -1 automatic
     int xalt = 0;                // register x pass with the half pencil tile
     int ytma = 1;                // register y passes with their tiles staged by TMA (0: plain loads)
+    int zstage = 1;              // register z passes stage their rows with bulk copies (0: element loads)
 };
 
 // Operator state for one arithmetic precision.  Owns its tables, the Green

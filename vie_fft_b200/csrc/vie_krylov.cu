@@ -518,6 +518,12 @@ template <typename C> struct ProBicgP {  // p = r + beta (p - omega v)
         const long long o = s * a + idx;
         return L{r[o], p[o], v[o], from_d2<C>(S[S_BETA]), from_d2<C>(S[S_OMEGA])};
     }
+    // r and v staged by the forward z pass (p is also written here, so it is read per element)
+    static constexpr int NSTAGE = 2;
+    __device__ __forceinline__ const C* stage_src(int k) const { return k ? v : r; }
+    __device__ __forceinline__ L load_staged(int s, long long idx, const C* sv) const {
+        return L{sv[0], p[s * a + idx], sv[1], from_d2<C>(S[S_BETA]), from_d2<C>(S[S_OMEGA])};
+    }
     __device__ __forceinline__ C apply(int s, long long idx, const L& l) const {
         const C pv = cadd(l.r, cmul(l.beta, csub(l.p, cmul(l.omega, l.v))));
         p[s * a + idx] = pv;
@@ -535,6 +541,11 @@ template <typename C> struct ProBicgS {  // s = r - alpha v
     __device__ __forceinline__ L load(int s, long long idx) const {
         const long long o = s * a + idx;
         return L{r[o], v[o], from_d2<C>(S[S_ALPHA])};
+    }
+    static constexpr int NSTAGE = 2;
+    __device__ __forceinline__ const C* stage_src(int k) const { return k ? v : r; }
+    __device__ __forceinline__ L load_staged(int, long long, const C* sv) const {
+        return L{sv[0], sv[1], from_d2<C>(S[S_ALPHA])};
     }
     __device__ __forceinline__ C apply(int s, long long idx, const L& l) const {
         const C x = csub(l.r, cmul(l.alpha, l.v));

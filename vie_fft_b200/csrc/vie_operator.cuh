@@ -69,6 +69,7 @@ template <typename C> struct OpDev {
     C* c;                      // 3 * nx*2ny*2nz scratch
     Gate gate;                 // launch gate of the current solve (state == nullptr: always run)
     int* status;               // device word set by a kernel whose bounded wait ran out (TMA staging)
+    int zstage;                // register z passes stage their rows with bulk copies (0: element loads)
 };
 
 __host__ __device__ inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
@@ -363,6 +364,9 @@ template <typename C> struct ProCopy {
     const C* __restrict__ x;
     long long a;
     struct L { C x; };
+    static constexpr int NSTAGE = 1;
+    __device__ __forceinline__ const C* stage_src(int) const { return x; }
+    __device__ __forceinline__ L load_staged(int, long long, const C* v) const { return L{v[0]}; }
     __device__ __forceinline__ L load(int s, long long idx) const { return L{x[s * a + idx]}; }
     __device__ __forceinline__ C apply(int, long long, const L& l) const { return l.x; }
     __device__ __forceinline__ C operator()(int s, long long idx, bool) const { return x[s * a + idx]; }
