@@ -56,6 +56,8 @@ TileCfg tiles_from_env() {
     if (const char* x = std::getenv("VIE_TMA")) t.ytma = std::atoi(x) == 0 ? 0 : 1;
     // VIE_ZSTAGE=0: the z passes with element loads instead of rows staged by bulk copies
     if (const char* x = std::getenv("VIE_ZSTAGE")) t.zstage = std::atoi(x) == 0 ? 0 : 1;
+    // VIE_WAIT_TEST=1: every staged tile's wait runs out (tests of VIE_ERR_TIMEOUT)
+    if (const char* x = std::getenv("VIE_WAIT_TEST")) t.wait_test = std::atoi(x) == 1 ? 1 : 0;
     return t;
 }
 

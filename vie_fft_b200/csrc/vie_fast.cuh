@@ -123,12 +123,15 @@ template <typename C, int TP> struct FastXLB {
 // mbarrier is bounded: after kTmaWaitIters polls the block records the failure
 // in op.status (mapped host memory, read by the host after the call), waits
 // once more (bounded) for the copy still in flight and leaves its tile undone.
+// op.wait_test makes that path run on purpose: the first wait then polls a
+// second mbarrier that nothing completes, kTestWaitIters times.
 constexpr int kTmaWaitIters = 1 << 22;
+constexpr int kTestWaitIters = 1 << 10;
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 
-__device__ __forceinline__ bool mbar_wait_bounded(unsigned bar, unsigned phase) {
-    for (int it = 0; it < kTmaWaitIters; it++) {
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned bar, unsigned phase, int limit = kTmaWaitIters) {
+    for (int it = 0; it < limit; it++) {
         unsigned ok;
         asm volatile(
             "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
@@ -140,10 +143,22 @@ __device__ __forceinline__ bool mbar_wait_bounded(unsigned bar, unsigned phase) 
     return false;
 }
 
-__device__ __forceinline__ void mbar_init_one(unsigned bar) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+// bars[0]: the staged tile's barrier; bars[1]: the one nothing completes (wait test)
+__device__ __forceinline__ void stage_init(unsigned long long* bars) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bars)) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bars + 1)) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+// the block's wait for its staged tile; false (for the whole block alike) when it
+// ran out, after the status word is set and the copy in flight is waited for
+__device__ __forceinline__ bool stage_ready(unsigned long long* bars, int wait_test, int* status) {
+    const bool ok = wait_test ? mbar_wait_bounded(smem_u32(bars + 1), 0, kTestWaitIters)
+                              : mbar_wait_bounded(smem_u32(bars), 0);
+    if (!__syncthreads_or(!ok)) return true;
+    if (threadIdx.x == 0 && status) *(volatile int*)status = 1;
+    mbar_wait_bounded(smem_u32(bars), 0);
+    return false;
 }
 __device__ __forceinline__ void mbar_expect(unsigned bar, unsigned bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
@@ -195,7 +210,7 @@ __global__ void __launch_bounds__(FastLB<C, N>::ROW, FastLB<C, N>::ROW_MIN) kf_f
     constexpr int NS = stage_count<Pro>::value;
     constexpr int ESZ = 2 * (R1 * (R2 + 1) > R2 * (R1 + 1) ? R1 * (R2 + 1) : R2 * (R1 + 1)) * ROWS;
     constexpr bool kCanStage = NS > 0 && NS * ROWS * N <= ESZ;
-    __shared__ __align__(8) unsigned long long zbar;
+    __shared__ __align__(8) unsigned long long zbar[2];
     bool staged = false;
     const long long row0 = (long long)blockIdx.x * ROWS;
     const int nr = (int)(nrows - row0 < ROWS ? nrows - row0 : ROWS);
@@ -203,23 +218,19 @@ __global__ void __launch_bounds__(FastLB<C, N>::ROW, FastLB<C, N>::ROW_MIN) kf_f
         staged = op.zstage != 0;
 #pragma unroll
         for (int k = 0; k < NS; k++) staged = staged && aligned16(pro.stage_src(k) + s * op.a + row0 * N);
-        if (staged && threadIdx.x == 0) mbar_init_one(smem_u32(&zbar));
+        if (staged && threadIdx.x == 0) stage_init(zbar);
     }
     __syncthreads();
     if constexpr (kCanStage) {
         if (staged) {
-            const unsigned b = smem_u32(&zbar);
+            const unsigned b = smem_u32(zbar);
             if (threadIdx.x == 0) {
                 const unsigned bytes = (unsigned)(sizeof(C) * N) * (unsigned)nr;
                 mbar_expect(b, bytes * NS);
 #pragma unroll
                 for (int k = 0; k < NS; k++) bulk_load(E + k * ROWS * N, pro.stage_src(k) + s * op.a + row0 * N, bytes, b);
             }
-            if (__syncthreads_or(!mbar_wait_bounded(b, 0))) {
-                if (threadIdx.x == 0 && op.status) *(volatile int*)op.status = 1;
-                mbar_wait_bounded(b, 0);
-                return;
-            }
+            if (!stage_ready(zbar, op.wait_test, op.status)) return;
         }
     }
     C v[R1];
@@ -343,25 +354,20 @@ __global__ void __launch_bounds__(FastLB<C, N>::ROW, FastLB<C, N>::ROW_MIN) kf_i
     const long long row = (long long)blockIdx.x * ROWS + r;
     const bool live = row < nrows;
     // the block's spectra rows (contiguous) staged whole into E by one bulk copy
-    __shared__ __align__(8) unsigned long long zbar;
+    __shared__ __align__(8) unsigned long long zbar[2];
     const long long row0 = (long long)blockIdx.x * ROWS;
     const int nr = (int)(nrows - row0 < ROWS ? nrows - row0 : ROWS);
     const C* bsrc = op.b + ((long long)s * nrows + row0) * (2 * N);
     const bool staged = op.zstage != 0 && aligned16(bsrc);
-    if (staged && threadIdx.x == 0) mbar_init_one(smem_u32(&zbar));
+    if (staged && threadIdx.x == 0) stage_init(zbar);
     __syncthreads();
     if (staged) {
-        const unsigned b = smem_u32(&zbar);
         if (threadIdx.x == 0) {
             const unsigned bytes = (unsigned)(sizeof(C) * 2 * N) * (unsigned)nr;
-            mbar_expect(b, bytes);
-            bulk_load(E, bsrc, bytes, b);
+            mbar_expect(smem_u32(zbar), bytes);
+            bulk_load(E, bsrc, bytes, smem_u32(zbar));
         }
-        if (__syncthreads_or(!mbar_wait_bounded(b, 0))) {
-            if (threadIdx.x == 0 && op.status) *(volatile int*)op.status = 1;
-            mbar_wait_bounded(b, 0);
-            return;
-        }
+        if (!stage_ready(zbar, op.wait_test, op.status)) return;
     }
     C X[2][R2];
     if (lane < R1 && live) {
@@ -525,7 +531,7 @@ __global__ void __launch_bounds__(FastLB<C, N>::COL, FastLB<C, N>::COL_MIN)
     if (gate_closed(op.gate)) return;
     constexpr int R1 = FastPlan<N>::R1, R2 = FastPlan<N>::R2, TP = FastTiles<C>::TP_Y;
     constexpr int HS = N * TP;
-    __shared__ __align__(8) unsigned long long bar;
+    __shared__ __align__(8) unsigned long long bar[2];
     C* tw;
     C* E = fast_smem<C, N>(op.ax[1].tw, tw);
     // the TMA destination 128-byte aligned (the launch reserves 128 more bytes)
@@ -534,16 +540,11 @@ __global__ void __launch_bounds__(FastLB<C, N>::COL, FastLB<C, N>::COL_MIN)
     const int Lz = 2 * op.nz;
     const int kz = blockIdx.x * TP + tx, i = blockIdx.y, s = blockIdx.z;
     const bool live = kz < Lz;
-    const unsigned b = smem_u32(&bar);
-    if (threadIdx.x == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b) : "memory");
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    }
+    const unsigned b = smem_u32(bar);
+    if (threadIdx.x == 0) stage_init(bar);
     __syncthreads();
     if (threadIdx.x == 0) {
-        const unsigned bytes = (unsigned)(sizeof(C) * N * TP);
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(bytes) : "memory");
+        mbar_expect(b, (unsigned)(sizeof(C) * N * TP));
         const int x = 2 * (int)blockIdx.x * TP;                    // reals
         const int y = ((int)blockIdx.z * op.nx + (int)blockIdx.y) * N;  // rows
         asm volatile(
@@ -551,14 +552,7 @@ __global__ void __launch_bounds__(FastLB<C, N>::COL, FastLB<C, N>::COL_MIN)
             ::"r"(smem_u32(E)), "l"(&tm), "r"(x), "r"(y), "r"(b)
             : "memory");
     }
-    // the whole block takes the same branch: a wait that ran out in any thread
-    // sets the status word, waits once more (bounded) for the copy in flight and
-    // leaves the pass undone
-    if (__syncthreads_or(!mbar_wait_bounded(b, 0))) {
-        if (threadIdx.x == 0 && op.status) *(volatile int*)op.status = 1;
-        mbar_wait_bounded(b, 0);
-        return;
-    }
+    if (!stage_ready(bar, op.wait_test, op.status)) return;
     // inputs of this thread from the staged tile (row n = n2 + R2 n1, column tx)
     C v[R1];
     const int n2 = lane;
@@ -652,7 +646,7 @@ __global__ void __launch_bounds__(FastLB<C, N>::COL, FastLB<C, N>::COL_MIN)
     if (gate_closed(op.gate)) return;
     constexpr int R1 = FastPlan<N>::R1, R2 = FastPlan<N>::R2, TP = FastTiles<C>::TP_Y;
     constexpr int HS = N * TP;
-    __shared__ __align__(8) unsigned long long bar;
+    __shared__ __align__(8) unsigned long long bar[2];
     C* tw;
     C* E = fast_smem<C, N>(op.ax[1].tw, tw);
     E = reinterpret_cast<C*>(reinterpret_cast<char*>(E) + ((128u - (smem_u32(E) & 127u)) & 127u));
@@ -660,16 +654,11 @@ __global__ void __launch_bounds__(FastLB<C, N>::COL, FastLB<C, N>::COL_MIN)
     const int Lz = 2 * op.nz;
     const int kz = blockIdx.x * TP + tx, i = blockIdx.y, s = blockIdx.z;
     const bool live = kz < Lz;
-    const unsigned b = smem_u32(&bar);
-    if (threadIdx.x == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b) : "memory");
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    }
+    const unsigned b = smem_u32(bar);
+    if (threadIdx.x == 0) stage_init(bar);
     __syncthreads();
     if (threadIdx.x == 0) {
-        const unsigned bytes = (unsigned)(sizeof(C) * 2 * N * TP);
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(bytes) : "memory");
+        mbar_expect(b, (unsigned)(sizeof(C) * 2 * N * TP));
         const int x = 2 * (int)blockIdx.x * TP;
         const int y = ((int)blockIdx.z * op.nx + (int)blockIdx.y) * 2 * N;
 #pragma unroll
@@ -680,14 +669,7 @@ __global__ void __launch_bounds__(FastLB<C, N>::COL, FastLB<C, N>::COL_MIN)
                 "l"(&tm), "r"(x), "r"(y + h * N), "r"(b)
                 : "memory");
     }
-    // the whole block takes the same branch: a wait that ran out in any thread
-    // sets the status word, waits once more (bounded) for the copy in flight and
-    // leaves the pass undone
-    if (__syncthreads_or(!mbar_wait_bounded(b, 0))) {
-        if (threadIdx.x == 0 && op.status) *(volatile int*)op.status = 1;
-        mbar_wait_bounded(b, 0);
-        return;
-    }
+    if (!stage_ready(bar, op.wait_test, op.status)) return;
     const int k1 = lane;
 #pragma unroll
     for (int h = 0; h < 2; h++) {

@@ -50,6 +50,7 @@ struct TileCfg {
     int xalt = 0;                // register x pass with the half pencil tile
     int ytma = 1;                // register y passes with their tiles staged by TMA (0: plain loads)
     int zstage = 1;              // register z passes stage their rows with bulk copies (0: element loads)
+    int wait_test = 0;           // 1: staged tiles' waits run out on purpose (timeout-path tests)
 };
 
 // Operator state for one arithmetic precision.  Owns its tables, the Green

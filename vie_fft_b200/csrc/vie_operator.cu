@@ -121,6 +121,7 @@ int Operator<T>::init(int nx, int ny, int nz, const double d[3], double k0, cons
         o.fast[ax] = (allow_fast && fast_length(n[ax]) && tiles.fast[ax] != 0) ? 1 : 0;
     o.xalt = tiles.xalt ? 1 : 0;
     o.zstage = tiles.zstage ? 1 : 0;
+    o.wait_test = tiles.wait_test ? 1 : 0;
 
     // ---- tables: per axis tw[2N], perm[N] (u16), P[2][2N], Q[2][2N], gfold[2N]
     size_t bytes = 0;

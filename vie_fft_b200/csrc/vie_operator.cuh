@@ -70,6 +70,7 @@ template <typename C> struct OpDev {
     Gate gate;                 // launch gate of the current solve (state == nullptr: always run)
     int* status;               // device word set by a kernel whose bounded wait ran out (TMA staging)
     int zstage;                // register z passes stage their rows with bulk copies (0: element loads)
+    int wait_test;             // 1: every staged tile's wait runs out on purpose (tests of the timeout path)
 };
 
 __host__ __device__ inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
