@@ -1,6 +1,7 @@
 """CUDA operator parity: Green spectrum, incident field, A x and A^H x in FP64
 and FP32 against the reference's outputs (golden fixtures from oracle/_ref)
 and the oracle restatement, plus size-independent properties at full sizes."""
+import ctypes
 import os
 
 import numpy as np
@@ -97,6 +98,78 @@ def test_matvec_fp32_matches_oracle(shape):
         c.matvec_dev(xt.data_ptr(), yt.data_ptr(), conj=True, precision=V.PREC_MIXED)
         c.sync()
         assert rel(yt.cpu().numpy(), refh) < FP32_TOL
+
+
+# the lengths the 128^3 and 256^3 grids run (register plans 16x8 and 16x16) in
+# each axis position: the x pass (both pencil tiles), the y passes with their
+# TMA-staged tiles (at 256 the inverse-y tile is two boxes of the maximum
+# height, 256 rows) and the z row passes, each against the oracle
+THIN = [(256, 6, 5), (5, 256, 6), (6, 5, 256), (128, 7, 9), (9, 128, 7), (7, 9, 128)]
+
+
+@pytest.mark.parametrize("shape", THIN)
+def test_lengths_128_256_match_oracle(shape, monkeypatch):
+    """A x and A^H x in FP64 (1e-12) and FP32 (2e-5, default and half x tile)
+    against the oracle (CG_Iteration.h:131-173, fft.h:41-127, 224-309)."""
+    torch = _torch()
+    rng = np.random.default_rng(sum(shape) + 7)
+    d = (0.01, 0.012, 0.011)
+    k0 = GEO.k0_of(530.0)
+    table = np.array([1.1, 2.4 - 0.05j, -8.5 - 0.3j, 3.8 - 0.6j])
+    mat = rng.integers(0, 4, size=shape).astype(np.uint8)
+    flags = rng.integers(0, 2, size=(3,) + shape).astype(np.uint8)
+    x = rng.standard_normal((3,) + shape) + 1j * rng.standard_normal((3,) + shape)
+    g = O.Grid(*shape, *d, k0)
+    G = O.green(g)
+    ref = [O.matvec(g, G, table[mat], flags, x, conj) for conj in (False, True)]
+    for xtile in ("0", "1"):
+        monkeypatch.setenv("VIE_XTILE", xtile)
+        with make_ctx(shape, d, k0, mat, flags, table) as c:
+            for conj in (False, True):
+                assert rel(c.matvec(x, conj), ref[conj]) < FP64_TOL, (xtile, conj)
+            xt = torch.from_numpy(x.astype(np.complex64)).cuda()
+            for conj in (False, True):
+                yt = torch.zeros_like(xt)
+                torch.cuda.synchronize()
+                c.matvec_dev(xt.data_ptr(), yt.data_ptr(), conj=conj, precision=V.PREC_MIXED)
+                c.sync()
+                assert rel(yt.cpu().numpy(), ref[conj]) < FP32_TOL, (xtile, conj)
+
+
+def test_green_block_256_matches_reference():
+    """One full-size self-term block, L_DC_Dq (fft.h:41-127) on the x current of
+    a seeded 256^3 field (two 512^3 transforms), against the reference's own
+    function built in place (oracle/_ref), else against the oracle restatement.
+    The GPU computes the block as the Green part of the operator on a vector
+    whose only non-zero component is x (the call dropin/fft.h makes).  On one
+    host core the reference takes about a minute for its Green's function and
+    the block; the GPU side takes under a second."""
+    n = (256, 256, 256)
+    d = (0.01, 0.01, 0.01)
+    k0 = GEO.k0_of(550.0)
+    table = np.array([1.1, 2.4 - 0.05j, 3.8 - 0.6j, -8.5 - 0.3j])
+    rng = np.random.default_rng(256)
+    x = np.zeros((3,) + n, np.complex128)
+    x[0] = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    g = O.Grid(*n, *d, k0)
+    if O.ref_available():
+        R = O.Reference(g, table)
+        R.L.ref_green(None)
+        ref = np.zeros(n, np.complex128)
+        assert R.L.ref_block(0, 0, 0, 0, O._p(x), O._p(ref)) == 0
+        R.release()
+    else:
+        G = O.green(g)
+        pad = np.zeros(tuple(2 * v for v in n), np.complex128)
+        pad[: n[0] - 1, : n[1], : n[2]] = x[0, : n[0] - 1]
+        ref = np.zeros(n, np.complex128)
+        O.lib().vo_block(ctypes.byref(g.c()), O._p(G), O._p(pad), O._p(ref))
+        del G, pad
+    mat = np.ones(n, np.uint8)
+    flags = np.ones((3,) + n, np.uint8)
+    with make_ctx(n, d, k0, mat, flags, table) as c:
+        y = c.apply(x, conj=False, parts=V.PART_GREEN)
+    assert rel(y[0], ref) < FP64_TOL
 
 
 # y lengths with register kernels; 2 nz not a multiple of the pencil tile width

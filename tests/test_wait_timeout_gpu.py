@@ -7,6 +7,8 @@ the block records the timeout in the status word, waits for its real copy to
 land and leaves its tile undone.  A context made afterwards without the switch
 computes the operator as before.
 """
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -15,6 +17,17 @@ from oracle import oracle as O
 from vie_fft_b200 import geometry as GEO
 
 pytestmark = pytest.mark.gpu
+
+
+def _static_matvec(c, x):
+    """vie_matvec_static through the C ABI: (status, y)."""
+    fn = V.lib().vie_matvec_static
+    fn.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), ctypes.c_int]
+    fn.restype = ctypes.c_int
+    x = np.ascontiguousarray(x, np.complex128)
+    y = np.zeros_like(x)
+    dp = ctypes.POINTER(ctypes.c_double)
+    return fn(c.handle, x.ctypes.data_as(dp), y.ctypes.data_as(dp), 0), y
 
 
 def _ctx(shape, mat, flags, table):
@@ -51,10 +64,17 @@ def test_wait_timeout_is_reported_and_device_stays_usable(monkeypatch):
         with pytest.raises(V.VieError) as e:
             c.solve("bicgstab", tol=1e-8, max_iter=2, allow_maxit=True)
         assert e.value.status == V.VIE_ERR_TIMEOUT
+        # the operator that allocates nothing stages the same z rows
+        rc, _ = _static_matvec(c, x)
+        assert rc == V.VIE_ERR_TIMEOUT
+        # the words were cleared by that call: the next call reports its own status only
+        assert V.lib().vie_sync(c.handle) == V.VIE_OK
     monkeypatch.delenv("VIE_WAIT_TEST")
 
     g = O.Grid(*shape, 0.01, 0.01, 0.01, GEO.k0_of(500.0))
     ref = O.matvec(g, O.green(g), table[mat], flags, x)
     with _ctx(shape, mat, flags, table) as c:
         y = c.matvec(x)
+        rc, ys = _static_matvec(c, x)
     assert np.abs(y - ref).max() < 1e-12 * np.abs(ref).max()
+    assert rc == V.VIE_OK and np.abs(ys - ref).max() < 1e-12 * np.abs(ref).max()

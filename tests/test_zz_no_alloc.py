@@ -37,6 +37,8 @@ def rel(a, b):
 
 
 def test_static_scratch_matvec_matches_allocating_matvec_twice():
+    torch = pytest.importorskip("torch")
+    assert torch.cuda.is_available(), "GPU tests need CUDA"
     w = GEO.single_sphere()  # 32^3: 12.6 MB of the 64 MiB scratch
     rng = np.random.default_rng(21)
     with V.Context(*w.shape, *w.d, w.k0) as c:
@@ -45,8 +47,14 @@ def test_static_scratch_matvec_matches_allocating_matvec_twice():
         c.green()
         for call, conj in enumerate((False, True)):
             x = rng.standard_normal((3,) + w.shape) + 1j * rng.standard_normal((3,) + w.shape)
+            # the second call is warm (kernels loaded, scratch address known):
+            # the device's free memory must not move across it
+            free0 = torch.cuda.mem_get_info(c.device)[0]
             rc, y = static_matvec(c, x, conj)
+            free1 = torch.cuda.mem_get_info(c.device)[0]
             assert rc == V.VIE_OK, (call, V.lib().vie_last_error(c.handle))
+            if call:
+                assert free1 == free0
             assert rel(y, c.matvec(x, conj=conj)) < FP64_TOL
 
 

@@ -153,6 +153,7 @@ class Context:
         self._L = lib()
         self.shape = (int(nx), int(ny), int(nz))
         self.a = int(nx) * int(ny) * int(nz)
+        self.device = int(device)
         g = VieGrid(int(nx), int(ny), int(nz), float(dx), float(dy), float(dz), float(k0), int(device))
         h = _vp()
         rc = self._L.vie_create(ctypes.byref(g), ctypes.byref(h))

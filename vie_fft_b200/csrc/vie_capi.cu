@@ -84,6 +84,7 @@ int ensure_operators(vie_ctx* ctx) {
 }
 
 int ready_for_operator(vie_ctx* ctx) {
+    if (int rc = ctx->check_usable()) return rc;
     if (!ctx->have_flags) return ctx->set_error(VIE_ERR_STATE, "edge flags not set (vie_set_flags)");
     if (!ctx->have_eps) return ctx->set_error(VIE_ERR_STATE, "permittivity not set (vie_set_material / vie_set_eps)");
     if (!ctx->have_green) return ctx->set_error(VIE_ERR_STATE, "Green's function not computed (vie_green)");
@@ -182,6 +183,7 @@ void vie_destroy(vie_ctx* ctx) {
 
 int vie_set_eps(vie_ctx* ctx, const double* eps) {
     if (check_ctx(ctx) || !eps) return VIE_ERR_ARG;
+    if (int u = ctx->check_usable()) return u;
     cudaSetDevice(ctx->device);
     // w = 1/(eps - 1), the per-voxel factor of the diagonal term (fft.h:430-432)
     for (long long v = 0; v < ctx->a; v++) {
@@ -201,6 +203,7 @@ int vie_set_material(vie_ctx* ctx, const uint8_t* material, const double* eps_re
                      int n_materials) {
     if (check_ctx(ctx) || !material || !eps_re || !eps_im || n_materials < 1 || n_materials > 256)
         return VIE_ERR_ARG;
+    if (int u = ctx->check_usable()) return u;
     std::vector<double> eps(2 * (size_t)ctx->a);
     for (long long v = 0; v < ctx->a; v++) {
         const int m = material[v];
@@ -214,6 +217,7 @@ int vie_set_material(vie_ctx* ctx, const uint8_t* material, const double* eps_re
 int vie_set_geometry_scene(vie_ctx* ctx, const vie_primitive* prims, int n, const double* eps_re,
                            const double* eps_im, int n_materials, uint8_t* material_out) {
     if (check_ctx(ctx) || !eps_re || !eps_im || n_materials < 1 || n_materials > 256) return VIE_ERR_ARG;
+    if (int u = ctx->check_usable()) return u;
     if (scene_check(prims, n)) return ctx->set_error(VIE_ERR_ARG, "invalid scene primitive (kind, label or parent)");
     for (int q = 0; q < n; q++)
         if (prims[q].label >= n_materials) return ctx->set_error(VIE_ERR_ARG, "scene label outside the table");
@@ -234,6 +238,7 @@ int vie_set_geometry_scene(vie_ctx* ctx, const vie_primitive* prims, int n, cons
 
 int vie_set_flags(vie_ctx* ctx, const uint8_t* fx, const uint8_t* fy, const uint8_t* fz) {
     if (check_ctx(ctx) || !fx || !fy || !fz) return VIE_ERR_ARG;
+    if (int u = ctx->check_usable()) return u;
     cudaSetDevice(ctx->device);
     std::vector<uint8_t> packed((size_t)ctx->a);
     for (long long v = 0; v < ctx->a; v++)
@@ -252,6 +257,7 @@ int vie_set_flags(vie_ctx* ctx, const uint8_t* fx, const uint8_t* fy, const uint
 
 int vie_green(vie_ctx* ctx) {
     if (check_ctx(ctx)) return VIE_ERR_ARG;
+    if (int u = ctx->check_usable()) return u;
     cudaSetDevice(ctx->device);
     int rc = green_compute(ctx);
     if (rc) return rc;
@@ -267,6 +273,7 @@ int vie_green(vie_ctx* ctx) {
 
 int vie_green_spectrum(vie_ctx* ctx, double* out) {
     if (check_ctx(ctx) || !out) return VIE_ERR_ARG;
+    if (int u = ctx->check_usable()) return u;
     if (!ctx->have_green) return ctx->set_error(VIE_ERR_STATE, "Green's function not computed (vie_green)");
     cudaSetDevice(ctx->device);
     const size_t m = 8 * (size_t)ctx->a;
@@ -284,6 +291,7 @@ int vie_green_spectrum(vie_ctx* ctx, double* out) {
 
 int vie_incident(vie_ctx* ctx, double theta, double phi, double psi, double* out) {
     if (check_ctx(ctx)) return VIE_ERR_ARG;
+    if (int u = ctx->check_usable()) return u;
     cudaSetDevice(ctx->device);
     int rc = incident_compute(ctx, theta, phi, psi, ctx->d_rhs);
     if (rc) return rc;
@@ -298,6 +306,7 @@ int vie_incident(vie_ctx* ctx, double theta, double phi, double psi, double* out
 
 int vie_set_rhs(vie_ctx* ctx, const double* e) {
     if (check_ctx(ctx) || !e) return VIE_ERR_ARG;
+    if (int u = ctx->check_usable()) return u;
     cudaSetDevice(ctx->device);
     CTX_CUDA(cudaMemcpyAsync(ctx->d_rhs, e, sizeof(double2) * 3 * (size_t)ctx->a, cudaMemcpyHostToDevice, ctx->stream));
     CTX_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -307,6 +316,7 @@ int vie_set_rhs(vie_ctx* ctx, const double* e) {
 
 int vie_rhs_device(vie_ctx* ctx, void** rhs) {
     if (check_ctx(ctx) || !rhs) return VIE_ERR_ARG;
+    if (int u = ctx->check_usable()) return u;
     *rhs = ctx->d_rhs;
     ctx->have_rhs = true;
     return VIE_OK;
@@ -356,6 +366,7 @@ int vie_apply(vie_ctx* ctx, const double* x, double* y, int conj, int parts) {
 
 int vie_reset(vie_ctx* ctx, double* v, int comp) {
     if (check_ctx(ctx) || !v || comp < 0 || comp > 2) return VIE_ERR_ARG;
+    if (int u = ctx->check_usable()) return u;
     if (!ctx->have_flags) return ctx->set_error(VIE_ERR_STATE, "edge flags not set (vie_set_flags)");
     cudaSetDevice(ctx->device);
     const size_t bytes = sizeof(double2) * (size_t)ctx->a;
@@ -437,6 +448,7 @@ int vie_power_grad(vie_ctx* ctx, const unsigned char* edge_mask, const vie_solve
 
 static int ready_for_post(vie_ctx* ctx) {
     if (check_ctx(ctx)) return VIE_ERR_ARG;
+    if (int u = ctx->check_usable()) return u;
     if (!ctx->have_x) return ctx->set_error(VIE_ERR_STATE, "no solution yet (vie_solve)");
     cudaSetDevice(ctx->device);
     return VIE_OK;
@@ -473,6 +485,7 @@ int vie_nearfield(vie_ctx* ctx, const uint8_t* material, double* ene_metal, doub
 
 int vie_autotune(vie_ctx* ctx, int flags, char* report, int report_len) {
     if (check_ctx(ctx)) return VIE_ERR_ARG;
+    if (int u = ctx->check_usable()) return u;
     if (!ctx->have_flags) return ctx->set_error(VIE_ERR_STATE, "edge flags not set (vie_set_flags)");
     cudaSetDevice(ctx->device);
     int rc = ensure_operators(ctx);

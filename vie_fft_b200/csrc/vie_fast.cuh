@@ -121,8 +121,11 @@ template <typename C, int TP> struct FastXLB {
 // ---------------------------------------------------------------------------
 // Asynchronous staging into shared memory (TMA unit).  Every wait on an
 // mbarrier is bounded: after kTmaWaitIters polls the block records the failure
-// in op.status (mapped host memory, read by the host after the call), waits
+// in op.status[0] (mapped host memory, read by the host after the call), waits
 // once more (bounded) for the copy still in flight and leaves its tile undone.
+// If that second wait runs out too, the copy may still write into shared
+// memory after the block has left, so the block also sets op.status[1]; the
+// host then marks the context unusable.
 // op.wait_test makes that path run on purpose: the first wait then polls a
 // second mbarrier that nothing completes, kTestWaitIters times.
 constexpr int kTmaWaitIters = 1 << 22;
@@ -157,7 +160,8 @@ __device__ __forceinline__ bool stage_ready(unsigned long long* bars, int wait_t
                               : mbar_wait_bounded(smem_u32(bars), 0);
     if (!__syncthreads_or(!ok)) return true;
     if (threadIdx.x == 0 && status) *(volatile int*)status = 1;
-    mbar_wait_bounded(smem_u32(bars), 0);
+    const bool landed = mbar_wait_bounded(smem_u32(bars), 0);
+    if (threadIdx.x == 0 && status && !landed) *(volatile int*)(status + 1) = 1;
     return false;
 }
 __device__ __forceinline__ void mbar_expect(unsigned bar, unsigned bytes) {

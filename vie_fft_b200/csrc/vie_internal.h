@@ -75,9 +75,9 @@ template <typename T> struct Operator {
     CUtensorMap tm_c{};          // TMA view of the c spectra for the inverse y pass
     bool tm_c_ok = false;
     const void* tm_c_addr = nullptr;
-    // set to 1 by a kernel whose bounded wait ran out: one word of mapped pinned
-    // host memory (h_status), so the host reads it after a synchronisation
-    // without a copy
+    // two words of mapped pinned host memory (h_status), so the host reads them
+    // after a synchronisation without a copy: [0] set by a kernel whose bounded
+    // wait ran out, [1] set when its copy had still not landed when it left
     int* h_status = nullptr;
     int* d_status = nullptr;
 
@@ -91,11 +91,15 @@ template <typename T> struct Operator {
     // y = A x (conj: A^H), plain store
     int apply(const C* x, C* y, bool conj, cudaStream_t st, Error& err);
     size_t scratch_bytes() const;
-    // true (and the word cleared) when a bounded device wait ran out since the last call
-    bool take_timeout() {
-        if (!h_status || !*(volatile int*)h_status) return false;
-        *(volatile int*)h_status = 0;
-        return true;
+    // since the last call: 0 no bounded device wait ran out, 1 one ran out (its
+    // tile left undone), 2 a copy was also still in flight when its block left;
+    // the words are cleared
+    int take_timeout() {
+        if (!h_status) return 0;
+        volatile int* s = h_status;
+        const int r = s[1] ? 2 : (s[0] ? 1 : 0);
+        s[0] = s[1] = 0;
+        return r;
     }
 };
 
@@ -178,6 +182,10 @@ struct vie_ctx {
     cudaStream_t stream_aux = nullptr;    // capture stream of conditional (IF) bodies
     cudaStream_t stream_parent = nullptr; // ctx->stream while an IF body is captured on stream_aux
 
+    // set when a staged copy was still in flight as its block left: shared
+    // memory of that SM may still be written, so nothing more is launched
+    bool unusable = false;
+
     int set_error(int code, const std::string& m) {
         err.code = code;
         err.msg = m;
@@ -186,8 +194,18 @@ struct vie_ctx {
     // after a synchronisation: VIE_ERR_TIMEOUT when a kernel's bounded wait on
     // its staged tile ran out since the last check (its pass was left undone)
     int check_waits(int rc) {
-        const bool t64 = op64.take_timeout(), t32 = op32.take_timeout();
+        const int t64 = op64.take_timeout(), t32 = op32.take_timeout();
+        if (t64 == 2 || t32 == 2) {
+            unusable = true;
+            return set_error(VIE_ERR_TIMEOUT, "a TMA copy was still in flight when its bounded waits ran out; "
+                                              "this context launches nothing more (destroy it)");
+        }
         if (t64 || t32) return set_error(VIE_ERR_TIMEOUT, "a TMA tile load did not complete within its bounded wait");
         return rc;
+    }
+    // VIE_ERR_TIMEOUT once check_waits has marked the context unusable
+    int check_usable() {
+        if (!unusable) return VIE_OK;
+        return set_error(VIE_ERR_TIMEOUT, "context unusable: an earlier call left a TMA copy in flight (destroy it)");
     }
 };

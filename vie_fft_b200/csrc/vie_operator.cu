@@ -207,8 +207,8 @@ int Operator<T>::init(int nx, int ny, int nz, const double d[3], double k0, cons
     o.c = d_c;
     // status word of the bounded waits, and the TMA view of b for the forward y pass
     if (!h_status) {
-        VIE_CUDA_TRY(cudaHostAlloc(&h_status, sizeof(int), cudaHostAllocMapped), err);
-        *h_status = 0;
+        VIE_CUDA_TRY(cudaHostAlloc(&h_status, 2 * sizeof(int), cudaHostAllocMapped), err);
+        h_status[0] = h_status[1] = 0;
         VIE_CUDA_TRY(cudaHostGetDevicePointer(&d_status, h_status, 0), err);
     }
     o.status = d_status;

@@ -61,6 +61,7 @@ int static_scratch_address(vie_ctx* ctx, void** out) {
 extern "C" int vie_matvec_static(vie_ctx* ctx, const double* x, double* y, int conj) {
     using namespace vie;
     if (!ctx || !x || !y) return VIE_ERR_ARG;
+    if (int u = ctx->check_usable()) return u;
     if (!ctx->have_flags) return ctx->set_error(VIE_ERR_STATE, "edge flags not set (vie_set_flags)");
     if (!ctx->have_eps) return ctx->set_error(VIE_ERR_STATE, "permittivity not set (vie_set_material / vie_set_eps)");
     if (!ctx->have_green) return ctx->set_error(VIE_ERR_STATE, "Green's function not computed (vie_green)");
@@ -94,9 +95,15 @@ extern "C" int vie_matvec_static(vie_ctx* ctx, const double* x, double* y, int c
     if (e != cudaSuccess) return ctx->set_error(VIE_ERR_CUDA, cudaGetErrorString(e));
     rc = launch_operator<double>(op, ProCopy<double2>{dx, a}, EpiStore<double2>{dy, a}, dx, conj != 0, nullptr,
                                  ctx->stream, ctx->err);
-    if (rc) return rc;
-    e = cudaMemcpyAsync(y, dy, bytes, cudaMemcpyDeviceToHost, ctx->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-    if (e != cudaSuccess) return ctx->set_error(VIE_ERR_CUDA, cudaGetErrorString(e));
-    return VIE_OK;
+    if (!rc) {
+        e = cudaMemcpyAsync(y, dy, bytes, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) rc = ctx->set_error(VIE_ERR_CUDA, cudaGetErrorString(e));
+    } else {
+        cudaStreamSynchronize(ctx->stream);  // the passes already enqueued finish before the status word is read
+    }
+    // the z passes stage their rows on bounded waits that report through the
+    // FP64 operator's status word (shared with this copy of the operator): a
+    // wait that ran out left part of y undone, which is an error of this call
+    return ctx->check_waits(rc);
 }

@@ -159,6 +159,12 @@ int time_apply(vie_ctx* ctx, Operator<T>& op, const cplx_t<T>* x, cplx_t<T>* y, 
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     *ms = t / reps;
+    // a schedule whose staged waits ran out was timed with tiles left undone:
+    // the tuning fails rather than pick it (the status words are cleared here)
+    if (const int w = op.take_timeout()) {
+        if (w == 2) ctx->unusable = true;
+        return ctx->set_error(VIE_ERR_TIMEOUT, "autotuner: a staged tile's bounded wait ran out while timing a schedule");
+    }
     return rc;
 }
 
