@@ -415,8 +415,37 @@ def run_gpu(args, rank, world, local_rank):
         "green_setup_s": green_s, "fft_schedule": schedule, "autotune_s": tune_s,
         "post_ms_gpu": post_ms,
     }
-    print(json.dumps(line), flush=True)
     c.close()
+    if world == 1 and args.workload == "c3" and not args.no_extras:
+        line["extras"] = extra_configs(args, rank, world, local_rank)
+    print(json.dumps(line), flush=True)
+
+
+def extra_configs(args, rank, world, local_rank):
+    """Summaries of the batched (C4) and adjoint-gradient (C5) workloads, run
+    after the headline measurement so that their figures are recorded with it:
+    one warm-up and one timed step each, C5 without its finite-difference pass
+    (tests/test_c5_fd_gpu.py holds that check)."""
+    ex = argparse.Namespace(**vars(args))
+    ex.steps, ex.warmup = 1, 1
+    ex.workload = "c4"
+    l4 = run_gpu_batch(ex, rank, world, local_rank, emit=False)
+    ex.workload = "c5"
+    l5 = run_gpu_gradient(ex, rank, world, local_rank, emit=False, fd_check=False)
+    return {
+        "note": "1 warm-up + 1 timed step each, host wall time of the batch / gradient call",
+        "c4": {"workload": l4["config"]["workload"], "instances": l4["config"]["instances"],
+               "instances_per_s_mixed": l4["value"], "instances_per_s_fp64": l4["fp64"]["instances_per_s"],
+               "speedup_mixed_vs_fp64": l4["speedup_mixed_vs_fp64"],
+               "xsec_max_rel_err_mixed_vs_fp64": l4["xsec_max_rel_err_mixed_vs_fp64"],
+               "iterations_min_max_mixed": l4["mixed"]["iterations_min_max"],
+               "failed": l4["mixed"]["failed"], "gpu_launches": l4["gpu_launches"]},
+        "c5": {"workload": l5["config"]["workload"], "gradients_per_s_mixed": l5["value"],
+               "gradients_per_s_fp64": l5["fp64"]["gradients_per_s"],
+               "speedup_mixed_vs_fp64": l5["speedup_mixed_vs_fp64"],
+               "grad_rel_diff_mixed_vs_fp64": l5["grad_rel_diff_mixed_vs_fp64"],
+               "power_rel_diff_mixed_vs_fp64": l5["power"]["rel_diff"], "gpu_launches": l5["gpu_launches"]},
+    }
 
 
 def batch_workloads(name):
@@ -434,7 +463,7 @@ def batch_workloads(name):
     return sweep + spheres, " + ".join(desc) + "; BiCGSTAB to rel-res 1e-8, one CUDA graph launch per batch"
 
 
-def run_gpu_batch(args, rank, world, local_rank):
+def run_gpu_batch(args, rank, world, local_rank, emit=True):
     """Batched solve: every instance in one vie_solve_batch call (one graph
     launch).  value = instances / batch time (mixed precision); the FP64 batch
     of the same instances gives the speed-up and the accuracy figures."""
@@ -501,13 +530,14 @@ def run_gpu_batch(args, rank, world, local_rank):
         "gpu_launches": launches, "clocks": clocks, "setup_s": setup_s,
         "device_bytes": torch.cuda.mem_get_info()[1] - torch.cuda.mem_get_info()[0],
     }
-    if rank == 0:
+    if rank == 0 and emit:
         print(json.dumps(line), flush=True)
     for c in ctxs:
         c.close()
+    return line
 
 
-def run_gpu_gradient(args, rank, world, local_rank):
+def run_gpu_gradient(args, rank, world, local_rank, emit=True, fd_check=True):
     """Adjoint gradient of the active-layer absorption summed over 450, 550 and
     650 nm (x-polarised) on the 128x128x64 design stack (64x64x32 design
     region, seed 5).  value = gradient evaluations/s with mixed-precision forward
@@ -559,7 +589,39 @@ def run_gpu_gradient(args, rank, world, local_rank):
     p64, g64, it64 = evaluate(V.PREC_FP64, TOL)
     torch.cuda.synchronize()
     t64 = time.perf_counter() - t0
-    # central differences of the FP64 objective at 32 design voxels
+    fd = None
+    if fd_check:
+        fd = fd_check_c5(ws, ctxs, mask, evaluate)
+    line = {
+        "metric": "adjoint gradient evaluations/s (absorbed power in the active layer, 3 wavelengths, "
+                  "forward + adjoint solves to rel-res 1e-8)",
+        "value": 1.0 / t_mixed, "unit": "gradients/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t_mixed * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "c64 inner + c128 refine", "data": "synthetic",
+        "config": {"workload": "128x128x64 solar-cell stack, 64x64x32 design region (eps Re[1,4] Im[0,0.5], "
+                               "seed 5), 450/550/650 nm x-pol, objective = NearField Ene_Active sum",
+                   "design_voxels": int(ws[0].meta["region"].sum())},
+        "fp64": {"gradients_per_s": 1.0 / t64, "iterations_fwd_adj": it64},
+        "mixed": {"iterations_fwd_adj": itm},
+        "speedup_mixed_vs_fp64": t64 / t_mixed,
+        "power": {"mixed": pm, "fp64": p64, "rel_diff": abs(pm - p64) / abs(p64)},
+        "grad_rel_diff_mixed_vs_fp64": float(np.abs(gm - g64).max() / np.abs(g64).max()),
+        "fd_check": fd,
+        "gpu_launches": launches, "clocks": clocks,
+    }
+    if rank == 0 and emit:
+        print(json.dumps(line), flush=True)
+    for c in ctxs:
+        c.close()
+    return line
+
+
+def fd_check_c5(ws, ctxs, mask, evaluate):
+    """Central differences of the FP64 objective at 32 seeded design voxels
+    (the same check as tests/test_c5_fd_gpu.py, over the three wavelengths)."""
+    import numpy as np
+
+    import vie_fft_b200 as V
     region = np.argwhere(ws[0].meta["region"])
     rng = np.random.default_rng(6)
     picks = [tuple(region[i]) for i in rng.choice(len(region), 32, replace=False)]
@@ -586,29 +648,8 @@ def run_gpu_gradient(args, rank, world, local_rank):
     worst = max(errs)
     for w, c in zip(ws, ctxs):
         c.set_eps(w.eps_voxel)
-    line = {
-        "metric": "adjoint gradient evaluations/s (absorbed power in the active layer, 3 wavelengths, "
-                  "forward + adjoint solves to rel-res 1e-8)",
-        "value": 1.0 / t_mixed, "unit": "gradients/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": t_mixed * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "c64 inner + c128 refine", "data": "synthetic",
-        "config": {"workload": "128x128x64 solar-cell stack, 64x64x32 design region (eps Re[1,4] Im[0,0.5], "
-                               "seed 5), 450/550/650 nm x-pol, objective = NearField Ene_Active sum",
-                   "design_voxels": int(ws[0].meta["region"].sum())},
-        "fp64": {"gradients_per_s": 1.0 / t64, "iterations_fwd_adj": it64},
-        "mixed": {"iterations_fwd_adj": itm},
-        "speedup_mixed_vs_fp64": t64 / t_mixed,
-        "power": {"mixed": pm, "fp64": p64, "rel_diff": abs(pm - p64) / abs(p64)},
-        "grad_rel_diff_mixed_vs_fp64": float(np.abs(gm - g64).max() / np.abs(g64).max()),
-        "fd_check": {"voxels": 32, "h": h, "solve_tol": fd_tol,
-                     "max_abs_err_over_max_grad": worst, "median_abs_err_over_max_grad": float(np.median(errs)),
-                     "max_grad": scale},
-        "gpu_launches": launches, "clocks": clocks,
-    }
-    if rank == 0:
-        print(json.dumps(line), flush=True)
-    for c in ctxs:
-        c.close()
+    return {"voxels": 32, "h": h, "solve_tol": fd_tol, "max_abs_err_over_max_grad": worst,
+            "median_abs_err_over_max_grad": float(np.median(errs)), "max_grad": scale}
 
 
 def main():
@@ -625,6 +666,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--fp64-iters", type=int, default=0)
     ap.add_argument("--no-autotune", action="store_true", help="keep the default FFT schedule")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="c3: skip the C4 / C5 summaries appended to the line")
     ap.add_argument("--only-matvec", action="store_true",
                     help="time operator applications only (FP32 and FP64), no solve")
     args = ap.parse_args()

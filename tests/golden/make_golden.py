@@ -21,6 +21,12 @@ Fixtures
                      reference on seeded currents of the small cases
   dropin_blocks.npz  X/Y/Z_FFT rows, L_DC_Dq, L_Dq, L??_DO (and conjugate
                      twins) and Current_Reset on small seeded cases
+  c2_<solver>.npz    the 128^3 cluster of 40 gold spheres (background eps 1.77
+                     mapped to vacuum) solved by the reference's CORS_FFT and
+                     BICGSTAB_FFT to 1e-8 and BICGSTAB_FFT to 1e-12: step
+                     count, last error, the field at 8192 seeded entries, two
+                     seeded random projections and the norm of the field,
+                     FarField1's forward value and the metal absorption
   dropin_program.npz the reference's unchanged main program (CG_FFT_VIE.cpp,
                      41 wavelengths) on the synthetic material tables of
                      program_tables(): its Ene_Metal, Ene_Active, Grid and
@@ -117,6 +123,47 @@ def make_c1():
     mask = w.flags.astype(bool)
     np.savez_compressed(os.path.join(OUT, "c1_sphere.npz"), steps=steps, err=err, x_flagged=x[mask],
                         forward_rcs=fwd, ext_over_cs=ext, metal_abs_over_cs=metal)
+
+
+# C2: (driver, CG_THR) of each fixture
+C2_RUNS = {"cors": ("cors", 1e-8), "bicgstab": ("bicgstab", 1e-8), "bicgstab_tight": ("bicgstab", 1e-12)}
+C2_SAMPLES = 8192
+
+
+def c2_probe(x):
+    """Size-independent summary of a C2 field (shared with the tests): the
+    field at seeded entries, two seeded random complex projections, the norm."""
+    flat = np.ascontiguousarray(x, np.complex128).ravel()
+    rng = np.random.default_rng(22)
+    idx = np.sort(rng.choice(flat.size, size=C2_SAMPLES, replace=False))
+    proj = []
+    for _ in range(2):
+        wv = rng.standard_normal(flat.size) + 1j * rng.standard_normal(flat.size)
+        proj.append(np.vdot(wv, flat))
+    return idx, flat[idx], np.array(proj), float(np.linalg.norm(flat))
+
+
+def make_c2(which):
+    """One C2 fixture (about 20-40 minutes of one host core for each run)."""
+    import time
+    solver, thr = C2_RUNS[which]
+    w = G.sphere_cluster()
+    g = O.Grid(*w.shape, *w.d, w.k0)
+    R = O.Reference(g, w.eps_table, w.theta, w.phi, w.psi)
+    R.set_geometry(w.material, w.flags)
+    R.green()
+    R.incident()
+    t = time.perf_counter()
+    x, steps, err = R.solve(solver, thr)
+    secs = time.perf_counter() - t
+    R.release()
+    idx, samples, proj, norm = c2_probe(x)
+    fwd = O.farfield1(g, x)
+    metal, _, _ = O.absorption(g, x, w.eps, w.material)
+    np.savez_compressed(os.path.join(OUT, f"c2_{which}.npz"), steps=steps, err=err, thr=thr, idx=idx,
+                        samples=samples, proj=proj, norm=norm, forward_rcs=fwd, metal=metal,
+                        reference_seconds=secs)
+    print(f"c2 {which}: {steps} steps, err {err:.3e}, {secs:.0f} s")
 
 
 GEOMETRY_CASES = [
@@ -244,6 +291,9 @@ if __name__ == "__main__":
         make_dropin_blocks()
     if "program" in which:
         make_dropin_program()
+    for k in C2_RUNS:
+        if f"c2_{k}" in which:
+            make_c2(k)
     for f in sorted(os.listdir(OUT)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(OUT, f)))

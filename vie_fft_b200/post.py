@@ -1,11 +1,13 @@
-"""Cross sections from a solved current (host side, numpy).
+"""Cross sections from a solved current, restated in numpy on the host.
 
-The reference computes these in NearFar.h after the solve, on the host:
-extinction from the forward-scattering amplitude (FarField1, NearFar.h:16-109)
-and absorption from the edge currents (NearField, NearFar.h:180-250).  They
-stay on the host in the drop-in design; this module restates them for
-reporting (bench.py's cross-section errors between the mixed and the FP64
-solves).
+The reference computes these in NearFar.h after the solve: extinction from
+the forward-scattering amplitude (FarField1, NearFar.h:16-109) and absorption
+from the edge currents (NearField, NearFar.h:180-250).  The library computes
+them on the GPU from the solution in device memory (vie_farfield1,
+vie_farfield2, vie_nearfield; Context.farfield1 / farfield2 / nearfield).
+This module is the host restatement: the edge masks of the adjoint objective
+(edge_mask) and bench.py's comparison of the mixed and FP64 solves' cross
+sections on fields copied to the host.
 """
 from __future__ import annotations
 
