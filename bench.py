@@ -439,12 +439,15 @@ def extra_configs(args, rank, world, local_rank):
                "speedup_mixed_vs_fp64": l4["speedup_mixed_vs_fp64"],
                "xsec_max_rel_err_mixed_vs_fp64": l4["xsec_max_rel_err_mixed_vs_fp64"],
                "iterations_min_max_mixed": l4["mixed"]["iterations_min_max"],
+               "operator_GBps": l4["operator_GBps"],
                "failed": l4["mixed"]["failed"], "gpu_launches": l4["gpu_launches"]},
         "c5": {"workload": l5["config"]["workload"], "gradients_per_s_mixed": l5["value"],
                "gradients_per_s_fp64": l5["fp64"]["gradients_per_s"],
                "speedup_mixed_vs_fp64": l5["speedup_mixed_vs_fp64"],
                "grad_rel_diff_mixed_vs_fp64": l5["grad_rel_diff_mixed_vs_fp64"],
-               "power_rel_diff_mixed_vs_fp64": l5["power"]["rel_diff"], "gpu_launches": l5["gpu_launches"]},
+               "power_rel_diff_mixed_vs_fp64": l5["power"]["rel_diff"], "gpu_launches": l5["gpu_launches"],
+               "iterations_fwd_adj_mixed": l5["mixed"]["iterations_fwd_adj"],
+               "iterations_fwd_adj_fp64": l5["fp64"]["iterations_fwd_adj"]},
     }
 
 
@@ -514,6 +517,12 @@ def run_gpu_batch(args, rank, world, local_rank, emit=True):
                 xerr[k] = max(xerr[k], abs(a[k] - b[k]) / abs(b[k]))
     it = [r.info["iterations"] for r in res]
     it64 = [r.info["iterations"] for r in r64]
+    # operator bytes moved by the batch (algorithmic bytes of every FP32 and FP64
+    # application; the Krylov vector passes are not counted): a lower bound of
+    # the batch's HBM throughput
+    op_bytes = sum(r.info["matvecs_fp32"] * bytes_per_matvec(w.shape, 8) +
+                   r.info["matvecs_fp64"] * bytes_per_matvec(w.shape, 16) for w, r in zip(ws, res))
+    op_bytes64 = sum(r.info["matvecs_fp64"] * bytes_per_matvec(w.shape, 16) for w, r in zip(ws, r64))
     line = {
         "metric": "batched instances/s to rel-res 1e-8 (FP32 inner / FP64 refine, one graph launch per batch)",
         "value": value_all, "unit": "instances/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -527,6 +536,8 @@ def run_gpu_batch(args, rank, world, local_rank, emit=True):
         "mixed": {"iterations_min_max": [min(it), max(it)], "failed": sum(1 for r in res if r.status),
                   "graph_loops": res[0].info["graph_loops"]},
         "xsec_max_rel_err_mixed_vs_fp64": xerr,
+        "operator_GBps": {"mixed": op_bytes / t_mixed / 1e9, "fp64": op_bytes64 / t64 / 1e9,
+                          "note": "operator applications x algorithmic bytes / batch time (vector passes not counted)"},
         "gpu_launches": launches, "clocks": clocks, "setup_s": setup_s,
         "device_bytes": torch.cuda.mem_get_info()[1] - torch.cuda.mem_get_info()[0],
     }
