@@ -79,3 +79,47 @@ def test_batch_host_loop_and_errors(monkeypatch):
     finally:
         for c in ctxs:
             c.close()
+
+
+def register_instances():
+    """Instances whose three axes all run on the register kernels, the batches
+    the persistent multi-instance loop takes: a wavelength sweep on one 24x32x16
+    stack (one size class) and spheres of edges 16 and 24 (two more)."""
+    sweep = GEO.batch_sweep(shape=(24, 32, 16), n_wavelengths=3, spacer_nm=3.0, active_nm=8.0, nspheres=1,
+                            radius_nm=3.0, sphere_z_nm=(6.0, 6.0))
+    spheres = GEO.batch_spheres(count=5, edges=(16, 24), seed=7)
+    return sweep + spheres
+
+
+def test_persistent_batch_matches_single_solves(monkeypatch):
+    """Mixed BiCGSTAB over size classes as persistent kernels per pass
+    (VIE_BATCH_FUSED=1): every instance bit-identical to its single solve and
+    to the per-instance graph branches (the default), with a fixed number of
+    kernels per size class and pass."""
+    ws = register_instances()
+    ctxs = [ctx_for(w) for w in ws]
+    try:
+        monkeypatch.setenv("VIE_BATCH_FUSED", "1")
+        n0 = V.launch_count()
+        rb = V.solve_batch(ctxs, "bicgstab", tol=1e-8, precision=V.PREC_MIXED, raise_errors=False)
+        fused = V.launch_count() - n0
+        monkeypatch.delenv("VIE_BATCH_FUSED")
+        n0 = V.launch_count()
+        rb0 = V.solve_batch(ctxs, "bicgstab", tol=1e-8, precision=V.PREC_MIXED, raise_errors=False)
+        branches = V.launch_count() - n0
+        for c, r, r0 in zip(ctxs, rb, rb0):
+            assert r.info["graph_loops"] == 1
+            rs = c.solve("bicgstab", tol=1e-8, precision=V.PREC_MIXED)
+            assert r.status == rs.status == r0.status
+            for k in ("steps", "iterations", "outer", "matvecs_fp32", "matvecs_fp64"):
+                assert r.info[k] == rs.info[k] == r0.info[k], k
+            np.testing.assert_array_equal(r.x, rs.x)
+            np.testing.assert_array_equal(r0.x, rs.x)
+        assert len({r.info["steps"] for r in rb}) > 1
+        # per pass a fixed set of kernels per size class (3 classes here), whatever
+        # the number of instances in it; the branches launch per instance
+        passes = max(r.info["iterations"] for r in rb) + 1
+        assert fused <= 30 * 3 * passes < branches, (fused, passes, branches)
+    finally:
+        for c in ctxs:
+            c.close()

@@ -196,8 +196,11 @@ template <class P> struct stage_count<P, std::void_t<decltype(P::NSTAGE)>> { sta
 // F1 (row pass): forward z with padding fused into the load.
 // E layout: E[h][row][k1][n2], k1 stride R2 + 1 (conflict-free transposed reads).
 // ---------------------------------------------------------------------------
+// The pass bodies take their block coordinates as arguments: the kernels below
+// pass blockIdx, the persistent batch kernels (vie_batch.cu) the coordinates of
+// the virtual block they are at.  Every early return is taken by the whole block.
 template <typename C, int N, class Pro>
-__global__ void __launch_bounds__(FastLB<C, N>::ROW, FastLB<C, N>::ROW_MIN) kf_fwd_z(OpDev<C> op, Pro pro) {
+__device__ __forceinline__ void kf_fwd_z_blk(const OpDev<C>& op, const Pro& pro, const int bx, const int s) {
     if (gate_closed(op.gate)) return;
     constexpr int R1 = FastPlan<N>::R1, R2 = FastPlan<N>::R2, L = fast_lanes<C, N>(), ROWS = fast_rows<C, N>();
     constexpr int SR = R2 + 1;                 // padded row of E
@@ -205,9 +208,8 @@ __global__ void __launch_bounds__(FastLB<C, N>::ROW, FastLB<C, N>::ROW_MIN) kf_f
     C* tw;
     C* E = fast_smem<C, N>(op.ax[2].tw, tw);
     const int lane = threadIdx.x % L, r = threadIdx.x / L;
-    const int s = blockIdx.y;
     const long long nrows = (long long)op.nx * op.ny;
-    const long long row = (long long)blockIdx.x * ROWS + r;
+    const long long row = (long long)bx * ROWS + r;
     const bool live = row < nrows;
     // the prologue's source rows of this block staged whole into E (when they fit
     // and are 16-byte aligned), then read from shared memory
@@ -216,7 +218,7 @@ __global__ void __launch_bounds__(FastLB<C, N>::ROW, FastLB<C, N>::ROW_MIN) kf_f
     constexpr bool kCanStage = NS > 0 && NS * ROWS * N <= ESZ;
     __shared__ __align__(8) unsigned long long zbar[2];
     bool staged = false;
-    const long long row0 = (long long)blockIdx.x * ROWS;
+    const long long row0 = (long long)bx * ROWS;
     const int nr = (int)(nrows - row0 < ROWS ? nrows - row0 : ROWS);
     if constexpr (kCanStage) {
         staged = op.zstage != 0;
@@ -335,6 +337,10 @@ __global__ void __launch_bounds__(FastLB<C, N>::ROW, FastLB<C, N>::ROW_MIN) kf_f
         }
     }
 }
+template <typename C, int N, class Pro>
+__global__ void __launch_bounds__(FastLB<C, N>::ROW, FastLB<C, N>::ROW_MIN) kf_fwd_z(OpDev<C> op, Pro pro) {
+    kf_fwd_z_blk<C, N, Pro>(op, pro, blockIdx.x, blockIdx.y);
+}
 
 // ---------------------------------------------------------------------------
 // I1 (row pass): inverse z, crop, diagonal term, mask, epilogue.
@@ -342,9 +348,11 @@ __global__ void __launch_bounds__(FastLB<C, N>::ROW, FastLB<C, N>::ROW_MIN) kf_f
 // ---------------------------------------------------------------------------
 // (conj: the adjoint operator's diagonal coefficient; a run-time flag, the
 // two modes differ by one conjugation)
+// (gdx: the row blocks of a component, the stride of the reduction partials)
 template <typename C, int N, class Epi>
-__global__ void __launch_bounds__(FastLB<C, N>::ROW, FastLB<C, N>::ROW_MIN) kf_inv_z(OpDev<C> op, const C* __restrict__ xin, Epi epi,
-                                                double2* __restrict__ partial, int conj) {
+__device__ __forceinline__ void kf_inv_z_blk(const OpDev<C>& op, const C* __restrict__ xin, const Epi& epi,
+                                             double2* __restrict__ partial, const int conj, const int bx, const int s,
+                                             const int gdx) {
     if (gate_closed(op.gate)) return;
     using R = typename real_of<C>::type;
     constexpr int R1 = FastPlan<N>::R1, R2 = FastPlan<N>::R2, L = fast_lanes<C, N>(), ROWS = fast_rows<C, N>();
@@ -353,13 +361,12 @@ __global__ void __launch_bounds__(FastLB<C, N>::ROW, FastLB<C, N>::ROW_MIN) kf_i
     C* tw;
     C* E = fast_smem<C, N>(op.ax[2].tw, tw);
     const int lane = threadIdx.x % L, r = threadIdx.x / L;
-    const int s = blockIdx.y;
     const long long nrows = (long long)op.nx * op.ny;
-    const long long row = (long long)blockIdx.x * ROWS + r;
+    const long long row = (long long)bx * ROWS + r;
     const bool live = row < nrows;
     // the block's spectra rows (contiguous) staged whole into E by one bulk copy
     __shared__ __align__(8) unsigned long long zbar[2];
-    const long long row0 = (long long)blockIdx.x * ROWS;
+    const long long row0 = (long long)bx * ROWS;
     const int nr = (int)(nrows - row0 < ROWS ? nrows - row0 : ROWS);
     const C* bsrc = op.b + ((long long)s * nrows + row0) * (2 * N);
     const bool staged = op.zstage != 0 && aligned16(bsrc);
@@ -468,7 +475,12 @@ __global__ void __launch_bounds__(FastLB<C, N>::ROW, FastLB<C, N>::ROW_MIN) kf_i
             }
         }
     }
-    if constexpr (Epi::K > 0) block_reduce_store<KA>(acc, partial, (long long)blockIdx.y * gridDim.x + blockIdx.x);
+    if constexpr (Epi::K > 0) block_reduce_store<KA>(acc, partial, (long long)s * gdx + bx);
+}
+template <typename C, int N, class Epi>
+__global__ void __launch_bounds__(FastLB<C, N>::ROW, FastLB<C, N>::ROW_MIN) kf_inv_z(OpDev<C> op, const C* __restrict__ xin, Epi epi,
+                                                double2* __restrict__ partial, int conj) {
+    kf_inv_z_blk<C, N, Epi>(op, xin, epi, partial, conj, blockIdx.x, blockIdx.y, gridDim.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -476,7 +488,7 @@ __global__ void __launch_bounds__(FastLB<C, N>::ROW, FastLB<C, N>::ROW_MIN) kf_i
 // E layout: E[h][k1][n2][tx].
 // ---------------------------------------------------------------------------
 template <typename C, int N>
-__global__ void __launch_bounds__(FastLB<C, N>::COL, FastLB<C, N>::COL_MIN) kf_fwd_y(OpDev<C> op) {
+__device__ __forceinline__ void kf_fwd_y_blk(const OpDev<C>& op, const int bx, const int i, const int s) {
     if (gate_closed(op.gate)) return;
     constexpr int R1 = FastPlan<N>::R1, R2 = FastPlan<N>::R2, TP = FastTiles<C>::TP_Y;
     constexpr int HS = N * TP;
@@ -484,7 +496,7 @@ __global__ void __launch_bounds__(FastLB<C, N>::COL, FastLB<C, N>::COL_MIN) kf_f
     C* E = fast_smem<C, N>(op.ax[1].tw, tw);
     const int tx = threadIdx.x % TP, lane = threadIdx.x / TP;
     const int Lz = 2 * op.nz;
-    const int kz = blockIdx.x * TP + tx, i = blockIdx.y, s = blockIdx.z;
+    const int kz = bx * TP + tx;
     const bool live = kz < Lz;
     const C* src = op.b + ((long long)s * op.nx + i) * (long long)N * Lz;
     __syncthreads();
@@ -518,6 +530,10 @@ __global__ void __launch_bounds__(FastLB<C, N>::COL, FastLB<C, N>::COL_MIN) kf_f
             for (int k2 = 0; k2 < R2; k2++) dst[(long long)(h * N + k1 + R1 * k2) * Lz + kz] = X[k2];
         }
     }
+}
+template <typename C, int N>
+__global__ void __launch_bounds__(FastLB<C, N>::COL, FastLB<C, N>::COL_MIN) kf_fwd_y(OpDev<C> op) {
+    kf_fwd_y_blk<C, N>(op, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // F2 with its pencil tile staged by TMA: one cp.async.bulk.tensor load of the
@@ -595,7 +611,7 @@ __global__ void __launch_bounds__(FastLB<C, N>::COL, FastLB<C, N>::COL_MIN)
 
 // I2 (column pass): inverse y, crop.  E layout: E[h][n2][k1][tx].
 template <typename C, int N>
-__global__ void __launch_bounds__(FastLB<C, N>::COL, FastLB<C, N>::COL_MIN) kf_inv_y(OpDev<C> op) {
+__device__ __forceinline__ void kf_inv_y_blk(const OpDev<C>& op, const int bx, const int i, const int s) {
     if (gate_closed(op.gate)) return;
     constexpr int R1 = FastPlan<N>::R1, R2 = FastPlan<N>::R2, TP = FastTiles<C>::TP_Y;
     constexpr int HS = N * TP;
@@ -603,7 +619,7 @@ __global__ void __launch_bounds__(FastLB<C, N>::COL, FastLB<C, N>::COL_MIN) kf_i
     C* E = fast_smem<C, N>(op.ax[1].tw, tw);
     const int tx = threadIdx.x % TP, lane = threadIdx.x / TP;
     const int Lz = 2 * op.nz;
-    const int kz = blockIdx.x * TP + tx, i = blockIdx.y, s = blockIdx.z;
+    const int kz = bx * TP + tx;
     const bool live = kz < Lz;
     const C* src = op.c + ((long long)s * op.nx + i) * (long long)(2 * N) * Lz;
     __syncthreads();
@@ -638,6 +654,10 @@ __global__ void __launch_bounds__(FastLB<C, N>::COL, FastLB<C, N>::COL_MIN) kf_i
             dst[(long long)n * Lz + kz] = cadd(y0[n1], cmulc(y1[n1], tw[n]));
         }
     }
+}
+template <typename C, int N>
+__global__ void __launch_bounds__(FastLB<C, N>::COL, FastLB<C, N>::COL_MIN) kf_inv_y(OpDev<C> op) {
+    kf_inv_y_blk<C, N>(op, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // I2 with its tile staged by TMA: the [2N rows x TP columns] spectra tile as two
@@ -719,7 +739,7 @@ __global__ void __launch_bounds__(FastLB<C, N>::COL, FastLB<C, N>::COL_MIN)
 // ---------------------------------------------------------------------------
 // (conj: the adjoint operator's tables and conj(Gs); a run-time flag)
 template <typename C, int N, int TP>
-__global__ void __launch_bounds__(FastXLB<C, TP>::XT, FastXLB<C, TP>::X_MIN) kf_x_spectral(OpDev<C> op, int conj) {
+__device__ __forceinline__ void kf_x_spectral_blk(const OpDev<C>& op, const int conj, const int bx, const int ky) {
     if (gate_closed(op.gate)) return;
     using R = typename real_of<C>::type;
     constexpr int R1 = FastPlan<N>::R1, R2 = FastPlan<N>::R2;
@@ -729,10 +749,9 @@ __global__ void __launch_bounds__(FastXLB<C, TP>::XT, FastXLB<C, TP>::X_MIN) kf_
     C* tw;
     C* E = fast_smem<C, N>(op.ax[0].tw, tw);
     const int Lz = 2 * op.nz, Ly = 2 * op.ny;
-    const int ky = blockIdx.y;
     const long long cs = (long long)Ly * Lz;
     const int tx = threadIdx.x % TP;
-    const int kz = blockIdx.x * TP + tx;
+    const int kz = bx * TP + tx;
     const bool live = kz < Lz;
     __syncthreads();
     // step A: thread (tx, s, n2)
@@ -826,6 +845,10 @@ __global__ void __launch_bounds__(FastXLB<C, TP>::XT, FastXLB<C, TP>::X_MIN) kf_
             }
         }
     }
+}
+template <typename C, int N, int TP>
+__global__ void __launch_bounds__(FastXLB<C, TP>::XT, FastXLB<C, TP>::X_MIN) kf_x_spectral(OpDev<C> op, int conj) {
+    kf_x_spectral_blk<C, N, TP>(op, conj, blockIdx.x, blockIdx.y);
 }
 
 template <typename C, int N, int TP = FastTiles<C>::TP_X> constexpr int fast_x_threads() {
