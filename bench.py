@@ -42,10 +42,18 @@ sys.path.insert(0, ROOT)
 
 METRIC = "solves/s & matvec ms to rel-res 1e-8: mixed vs FP64 on 1 B200; % HBM peak"
 TOL = 1e-8
-# BiCGSTAB iterations of the FP64 solve of these workloads to 1e-8 on the GPU
-# (measured; the 256^3 value is the mean over four right-hand sides perturbed
-# at rounding level, 453-477; used only to scale the CPU sample to solves/s)
-FP64_ITERS = {"c3": 468, "c2": 21, "c1": 36}
+# the 32^3 sphere is solved to 1e-6, as the reference's CPU case is specified
+WORKLOAD_TOL = {"c1": 1e-6}
+# BiCGSTAB iterations of the FP64 solve of these workloads to their tolerance
+# (the 256^3 and 128^3 values measured on the GPU, the 256^3 one the mean over
+# four right-hand sides perturbed at rounding level, 453-477; the 32^3 value is
+# the reference's own step count at 1e-6); used only to scale the CPU sample to
+# solves/s
+FP64_ITERS = {"c3": 472, "c2": 21, "c1": 23}
+
+
+def tol_of(name):
+    return WORKLOAD_TOL.get(name, TOL)
 
 
 def workload(name):
@@ -68,7 +76,8 @@ def workload(name):
         return G.sphere_cluster(), "128^3 cluster of 40 Au spheres (r 5-15 nm, seed 2) in eps_b=1.77, 1 nm voxels, " \
                                    "padded 256^3, x-pol 500 nm, BiCGSTAB to rel-res 1e-8"
     if name == "c1":
-        return G.single_sphere(), "32^3 Ag sphere r=18 nm, 1.25 nm voxels, padded 64^3, x-pol 400 nm"
+        return G.single_sphere(), "32^3 Ag sphere r=18 nm, 1.25 nm voxels, padded 64^3, x-pol 400 nm, " \
+                                  "BiCGSTAB to rel-res 1e-6"
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -165,6 +174,12 @@ def cpu_solves_per_s(block_seconds, iters):
     return 1.0 / (block_seconds * 9 * 2 * iters)
 
 
+def workload_config(w, desc, tol=TOL):
+    """The workload both arms time: grid, padding, driver and tolerance."""
+    return {"workload": desc, "grid": list(w.shape), "padded": [2 * s for s in w.shape], "solver": "bicgstab",
+            "tol": tol}
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -188,7 +203,9 @@ def run_reference(args, rank, world):
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": block * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-            "config": {"workload": desc, "grid": list(w.shape), "parallelism": "processes"},
+            "config": workload_config(w, desc, tol_of(args.workload)),
+            "arm": {"precision": "c128 (the reference's double-complex path on the MKL shim)",
+                    "parallelism": f"{procs} host processes"},
             "cpu_baseline": {"value": value, "unit": "solves/s", "cores": procs, "kind": kind,
                              "sample": f"one L_DC_Dq block (two {2*w.shape[0]}^3 FFTs + multiply + crop) per "
                                        f"process, {procs} processes; solves/s = procs / (block_s * 9 blocks * "
@@ -240,7 +257,7 @@ def run_gpu(args, rank, world, local_rank):
             dist.barrier()
 
     def solve(precision, true_residual=False, out=None):
-        r = c.solve("bicgstab", tol=TOL, precision=precision, copy=out is not None, out=out,
+        r = c.solve("bicgstab", tol=tol_of(args.workload), precision=precision, copy=out is not None, out=out,
                     true_residual=true_residual)
         return r
 
@@ -349,7 +366,7 @@ def run_gpu(args, rank, world, local_rank):
         f0.record(stream)
         for _ in range(args.e2e_steps):
             c.set_rhs(h_rhs.numpy())
-            c.solve("bicgstab", tol=TOL, precision=V.PREC_MIXED, out=xn, true_residual=False)
+            c.solve("bicgstab", tol=tol_of(args.workload), precision=V.PREC_MIXED, out=xn, true_residual=False)
         f1.record(stream)
         f1.synchronize()
         wall = (time.perf_counter() - tw0) / args.e2e_steps
@@ -393,10 +410,10 @@ def run_gpu(args, rank, world, local_rank):
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "c64 inner + c128 refine", "data": "synthetic",
-        "config": {"workload": desc, "grid": list(w.shape), "padded": [2 * s for s in w.shape],
-                   "solver": "bicgstab", "tol": TOL, "precision": "mixed (FP32 inner Krylov, FP64 defect correction)",
-                   "l2": "inputs larger than L2 (FP32 vectors 403 MB, FP64 805 MB each)",
-                   "parallelism": "replicas" if world > 1 else "single"},
+        "config": workload_config(w, desc, tol_of(args.workload)),
+        "arm": {"precision": "mixed (FP32 inner Krylov, FP64 reliable updates)",
+                "l2": "inputs larger than L2 (FP32 vectors 403 MB, FP64 805 MB each)",
+                "parallelism": "replicas" if world > 1 else "single"},
         "roofline": {"bound": "hbm", "achieved": ach32, "peak": peak, "unit": "GB/s", "frac": ach32 / peak,
                      "traffic": traffic, "kernel": "FP32 operator application (5 pruned FFT passes)",
                      "peak_source": peak_kind, "algorithmic_bytes": B32},
