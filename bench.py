@@ -3,13 +3,16 @@
 
 Workload (default ``c3``): 256^3 organic solar cell (PEDOT 40 nm, P3HT:PCBM
 120 nm, 16 Ag spheres r = 20 nm seeded in the active layer), 1 nm voxels,
-padded 512^3, x-polarised plane wave at 550 nm, BiCGSTAB to relative
-residual 1e-8 from x0 = 0.  Synthetic geometry from vie_fft_b200.geometry.
+padded 512^3, x-polarised plane wave at 550 nm, the reference's CORS driver
+(CORS_FFT) to relative residual 1e-8 from x0 = 0.  Synthetic geometry from
+vie_fft_b200.geometry.
 
-One step = one full solve on inputs resident in HBM: FP32-complex inner
-BiCGSTAB inside FP64 defect correction (``value``, solves/s).  The all-FP64
-solve of the same system is timed after it for the speed-up, and the
-operator application (the hot op) is timed on its own for the roofline.
+One step = one full solve on inputs resident in HBM: FP32-complex inner CORS
+inside FP64 defect correction (``value``, solves/s).  The all-FP64 CORS solve
+of the same system is timed after it for the speed-up, and the operator
+application (the hot op) is timed on its own for the roofline.  ``extras``
+holds the same pair for BiCGSTAB (the reference's default driver) and short
+summaries of the batched (C4) and gradient (C5) workloads.
 
 ``e2e`` times the same solve through the C ABI with host buffers: every step
 copies the incident field from pinned host memory to the device and the
@@ -42,18 +45,25 @@ sys.path.insert(0, ROOT)
 
 METRIC = "solves/s & matvec ms to rel-res 1e-8: mixed vs FP64 on 1 B200; % HBM peak"
 TOL = 1e-8
-# the 32^3 sphere is solved to 1e-6, as the reference's CPU case is specified
+# the 32^3 sphere is solved to 1e-6 by BiCGSTAB, as the reference's CPU case is
+# specified; the 128^3 and 256^3 lines time the reference's CORS driver (CORS_FFT,
+# CG_Iteration.h:780-1073), the fastest of its drivers to 1e-8 on these grids
+# (256^3 to 1e-8: FP64 CORS 4.98 s, BiCGSTAB 7.62 s; mixed CORS 2.47 s, mixed
+# BiCGSTAB 4.20 s), with the BiCGSTAB figures of the 256^3 case in `extras`
 WORKLOAD_TOL = {"c1": 1e-6}
-# BiCGSTAB iterations of the FP64 solve of these workloads to their tolerance
-# (the 256^3 and 128^3 values measured on the GPU, the 256^3 one the mean over
-# four right-hand sides perturbed at rounding level, 453-477; the 32^3 value is
-# the reference's own step count at 1e-6); used only to scale the CPU sample to
-# solves/s
-FP64_ITERS = {"c3": 472, "c2": 21, "c1": 23}
+WORKLOAD_SOLVER = {"c1": "bicgstab", "c2": "cors", "c3": "cors"}
+# iterations of the FP64 solve of these workloads (driver and tolerance above):
+# 256^3 CORS 279 and 128^3 CORS 17 measured on the GPU, 32^3 BiCGSTAB 24 the
+# reference's own (its 23 steps + 1); used only to scale the CPU sample to solves/s
+FP64_ITERS = {"c3": 279, "c2": 17, "c1": 24}
 
 
 def tol_of(name):
     return WORKLOAD_TOL.get(name, TOL)
+
+
+def solver_of(name):
+    return WORKLOAD_SOLVER.get(name, "bicgstab")
 
 
 def workload(name):
@@ -71,10 +81,10 @@ def workload(name):
         return w, f"synthetic {shape} operator (random metal voxels)"
     if name == "c3":
         return G.solar_cell(), "256^3 organic solar cell (PEDOT/P3HT:PCBM, 16 Ag spheres r=20nm), 1 nm voxels, " \
-                               "padded 512^3, x-pol 550 nm, BiCGSTAB to rel-res 1e-8"
+                               "padded 512^3, x-pol 550 nm, CORS to rel-res 1e-8"
     if name == "c2":
         return G.sphere_cluster(), "128^3 cluster of 40 Au spheres (r 5-15 nm, seed 2) in eps_b=1.77, 1 nm voxels, " \
-                                   "padded 256^3, x-pol 500 nm, BiCGSTAB to rel-res 1e-8"
+                                   "padded 256^3, x-pol 500 nm, CORS to rel-res 1e-8"
     if name == "c1":
         return G.single_sphere(), "32^3 Ag sphere r=18 nm, 1.25 nm voxels, padded 64^3, x-pol 400 nm, " \
                                   "BiCGSTAB to rel-res 1e-6"
@@ -170,13 +180,13 @@ def usable_cores(w):
 
 
 def cpu_solves_per_s(block_seconds, iters):
-    # one BiCGSTAB iteration = 2 operator applications = 2 x 9 blocks
+    # one BiCGSTAB or CORS iteration = 2 operator applications = 2 x 9 blocks
     return 1.0 / (block_seconds * 9 * 2 * iters)
 
 
-def workload_config(w, desc, tol=TOL):
+def workload_config(w, desc, tol=TOL, solver="bicgstab"):
     """The workload both arms time: grid, padding, driver and tolerance."""
-    return {"workload": desc, "grid": list(w.shape), "padded": [2 * s for s in w.shape], "solver": "bicgstab",
+    return {"workload": desc, "grid": list(w.shape), "padded": [2 * s for s in w.shape], "solver": solver,
             "tol": tol}
 
 
@@ -203,7 +213,7 @@ def run_reference(args, rank, world):
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": block * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-            "config": workload_config(w, desc, tol_of(args.workload)),
+            "config": workload_config(w, desc, tol_of(args.workload), solver_of(args.workload)),
             "arm": {"precision": "c128 (the reference's double-complex path on the MKL shim)",
                     "parallelism": f"{procs} host processes"},
             "cpu_baseline": {"value": value, "unit": "solves/s", "cores": procs, "kind": kind,
@@ -256,9 +266,9 @@ def run_gpu(args, rank, world, local_rank):
         if dist is not None:
             dist.barrier()
 
-    def solve(precision, true_residual=False, out=None):
-        r = c.solve("bicgstab", tol=tol_of(args.workload), precision=precision, copy=out is not None, out=out,
-                    true_residual=true_residual)
+    def solve(precision, true_residual=False, out=None, solver=None):
+        r = c.solve(solver or solver_of(args.workload), tol=tol_of(args.workload), precision=precision,
+                    copy=out is not None, out=out, true_residual=true_residual)
         return r
 
     if args.only_matvec:
@@ -366,7 +376,8 @@ def run_gpu(args, rank, world, local_rank):
         f0.record(stream)
         for _ in range(args.e2e_steps):
             c.set_rhs(h_rhs.numpy())
-            c.solve("bicgstab", tol=tol_of(args.workload), precision=V.PREC_MIXED, out=xn, true_residual=False)
+            c.solve(solver_of(args.workload), tol=tol_of(args.workload), precision=V.PREC_MIXED, out=xn,
+                    true_residual=False)
         f1.record(stream)
         f1.synchronize()
         wall = (time.perf_counter() - tw0) / args.e2e_steps
@@ -402,7 +413,7 @@ def run_gpu(args, rank, world, local_rank):
         iters64 = r64.info["iterations"]
         cpu = {"value": cpu_solves_per_s(blk, iters64), "unit": "solves/s", "cores": 1, "kind": res[0]["kind"],
                "sample": f"one L_DC_Dq block at {w.shape} ({2*w.shape[0]}^3 padded FFT pair, {blk:.1f} s), "
-                         f"scaled by 9 blocks x 2 matvecs x {iters64} FP64 BiCGSTAB iterations",
+                         f"scaled by 9 blocks x 2 matvecs x {iters64} FP64 {solver_of(args.workload)} iterations",
                "block_seconds": blk}
 
     info = infos[-1]
@@ -410,7 +421,7 @@ def run_gpu(args, rank, world, local_rank):
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "c64 inner + c128 refine", "data": "synthetic",
-        "config": workload_config(w, desc, tol_of(args.workload)),
+        "config": workload_config(w, desc, tol_of(args.workload), solver_of(args.workload)),
         "arm": {"precision": "mixed (FP32 inner Krylov, FP64 reliable updates)",
                 "l2": "inputs larger than L2 (FP32 vectors 403 MB, FP64 805 MB each)",
                 "parallelism": "replicas" if world > 1 else "single"},
@@ -432,9 +443,26 @@ def run_gpu(args, rank, world, local_rank):
         "green_setup_s": green_s, "fft_schedule": schedule, "autotune_s": tune_s,
         "post_ms_gpu": post_ms,
     }
+    bicgstab = None
+    if world == 1 and args.workload == "c3" and not args.no_extras:
+        # the reference's default driver on the same system: mixed and FP64 BiCGSTAB
+        # (one warm-up solve each for the graph capture, then one timed)
+        bicgstab = {}
+        for name, prec in (("mixed", V.PREC_MIXED), ("fp64", V.PREC_FP64)):
+            solve(prec, solver="bicgstab")
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            rb = solve(prec, solver="bicgstab")
+            e1.record(stream)
+            e1.synchronize()
+            bicgstab[name] = {"solves_per_s": 1e3 / e0.elapsed_time(e1), "ms": e0.elapsed_time(e1),
+                              "iterations": rb.info["iterations"], "outer": rb.info["outer"]}
+        bicgstab["speedup_mixed_vs_fp64"] = bicgstab["fp64"]["ms"] / bicgstab["mixed"]["ms"]
+        bicgstab["speedup_mixed_cors_vs_fp64_bicgstab"] = bicgstab["fp64"]["ms"] / ms_max
     c.close()
     if world == 1 and args.workload == "c3" and not args.no_extras:
         line["extras"] = extra_configs(args, rank, world, local_rank)
+        line["extras"]["bicgstab_256"] = bicgstab
     print(json.dumps(line), flush=True)
 
 

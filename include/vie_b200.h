@@ -137,7 +137,7 @@ typedef struct {
     double tol;         /* relative-residual threshold (CG_THR, CG_Iteration.h:46) */
     int max_iter;       /* iteration cap; <= 0 means nx*ny*nz like the reference */
     double inner_tol;   /* mixed: residual reduction per FP64 refinement step
-                           (<= 0: 0.03 for BiCGSTAB's reliable updates, 1e-4 for the
+                           (<= 0: 0.03 for BiCGSTAB's reliable updates, 5e-5 for the
                            restarted inner solves of the other drivers) */
     int max_outer;      /* mixed: refinement cap (<= 0: 30) */
     int verbose;        /* print "CG Error" per iteration like the reference */
