@@ -658,21 +658,19 @@ static int solve_cors(vie_ctx* ctx, Operator<T>& op, const cplx_t<T>* b, cplx_t<
         // Ap = A r; rho = b^H Ap (:853-869)
         if ((rc2 = opmv(ctx, op, ProCopy<C>{r, a}, EpiDotB<C>{Ap, b, a}, r, false))) return rc2;
         if ((rc2 = finalize<1>(ctx, nblk, FinCorsRho{ctl}))) return rc2;
-        // p = r + beta pc; qc = Ap + beta rc; q = qc + beta rc + beta^2 q (:880-915);
-        // on the first step beta = 0 and pc = rc = q = 0: p = r, qc = q = Ap (:843-851)
-        if ((rc2 = lin(ctx, LinArgs<C, 2, 0>{p, 0, {{r, cs(-1)}, {pc, cs(S_BETA)}}, {}}))) return rc2;
-        if ((rc2 = lin(ctx, LinArgs<C, 2, 0>{qc, 0, {{Ap, cs(-1)}, {rc_, cs(S_BETA)}}, {}}))) return rc2;
-        if ((rc2 = lin(ctx, LinArgs<C, 3, 0>{q, 0, {{q, cs(S_T0)}, {rc_, cs(S_BETA)}, {qc, cs(-1)}}, {}}))) return rc2;
-        // Aq = A q; alpha = rho / (b^H Aq) (:938-962)
-        if ((rc2 = opmv(ctx, op, ProCopy<C>{q, a}, EpiDotB<C>{Aq, b, a}, q, false))) return rc2;
-        if ((rc2 = finalize<1>(ctx, nblk, FinCorsAlpha{}))) return rc2;
-        // pc = p - alpha q; rc = qc - alpha Aq (:964-981)
-        if ((rc2 = lin(ctx, LinArgs<C, 2, 0>{pc, 0, {{p, cs(-1)}, {q, cs(S_ALPHA, -1.0)}}, {}}))) return rc2;
-        if ((rc2 = lin(ctx, LinArgs<C, 2, 0>{rc_, 0, {{qc, cs(-1)}, {Aq, cs(S_ALPHA, -1.0)}}, {}}))) return rc2;
-        // x += 2 alpha p - alpha^2 q (:983-997); r += -2 alpha qc + alpha^2 Aq (:999-1012); r^H r
-        if ((rc2 = lin(ctx, LinArgs<C, 2, 0>{x, 1, {{p, cs(S_ALPHA, 2.0)}, {q, cs(S_T1, -1.0)}}, {}}))) return rc2;
-        if ((rc2 = lin(ctx, LinArgs<C, 2, 1>{r, 1, {{qc, cs(S_ALPHA, -2.0)}, {Aq, cs(S_T1)}}, {{nullptr, 1}}})))
+        // p = r + beta pc; qc = Ap + beta rc; q = qc + beta rc + beta^2 q (:880-915)
+        // in the first pass of Aq = A q; alpha = rho / (b^H Aq) (:938-962).  On the
+        // first step beta = 0 and pc = rc = q = 0: p = r, qc = q = Ap (:843-851)
+        if ((rc2 = opmv(ctx, op, ProCorsQ<C>{r, p, pc, Ap, qc, rc_, q, ctx->d_scal, a}, EpiDotB<C>{Aq, b, a}, q,
+                        false)))
             return rc2;
+        if ((rc2 = finalize<1>(ctx, nblk, FinCorsAlpha{}))) return rc2;
+        // pc = p - alpha q; rc = qc - alpha Aq (:964-981); x += 2 alpha p - alpha^2 q
+        // (:983-997); r += -2 alpha qc + alpha^2 Aq (:999-1012); r^H r: one pass
+        k_cors_update<C><<<kVecBlocks, 256, 0, ctx->stream>>>(pc, rc_, x, r, p, q, qc, Aq, n, ctx->d_scal,
+                                                               ctx->d_partial, ctx->gate);
+        count_launch();
+        VIE_CUDA_TRY(cudaGetLastError(), ctx->err);
         return finalize<1>(ctx, kVecBlocks, then(FinErr{}, DecideErr{ctl, hist}));
     };
     auto fin = [ctx, &res, verbose]() { return finish(ctx, res, 0, 2, PS_ERR_STEPS, verbose, "CORS"); };

@@ -573,6 +573,80 @@ template <typename C> struct EpiResidual {  // r = b - y; acc ||r||^2
     }
 };
 
+// CORS: the three vector updates after beta (CG_Iteration.h:880-915) as the
+// prologue of the forward z pass of A q, element by element exactly as the
+// separate passes compute them (k_lin: zero, then each term added in order):
+//   p = r + beta pc;  qc = Ap + beta rc;  q = beta^2 q + beta rc + qc (new qc)
+// and q (new) is the operator's source.  r and Ap are staged with the rows.
+template <typename C> struct ProCorsQ {
+    const C* __restrict__ r;
+    C* __restrict__ p;
+    const C* __restrict__ pc;
+    const C* __restrict__ Ap;
+    C* __restrict__ qc;
+    const C* __restrict__ rc;
+    C* __restrict__ q;
+    const double2* __restrict__ S;
+    long long a;
+    struct L { C r, pc, Ap, rc, q, one, beta, t0; };
+    __device__ __forceinline__ L coefs(C rv, C pcv, C apv, C rcv, C qv) const {
+        return L{rv, pcv, apv, rcv, qv, coef_c<C>(eval_coef(CoefSpec{-1, 1.0, 0.0}, S)),
+                 coef_c<C>(eval_coef(CoefSpec{S_BETA, 1.0, 0.0}, S)), coef_c<C>(eval_coef(CoefSpec{S_T0, 1.0, 0.0}, S))};
+    }
+    __device__ __forceinline__ L load(int s, long long idx) const {
+        const long long o = s * a + idx;
+        return coefs(r[o], pc[o], Ap[o], rc[o], q[o]);
+    }
+    static constexpr int NSTAGE = 2;
+    __device__ __forceinline__ const C* stage_src(int k) const { return k ? Ap : r; }
+    __device__ __forceinline__ L load_staged(int s, long long idx, const C* sv) const {
+        const long long o = s * a + idx;
+        return coefs(sv[0], pc[o], sv[1], rc[o], q[o]);
+    }
+    __device__ __forceinline__ C apply(int s, long long idx, const L& l) const {
+        const long long o = s * a + idx;
+        const C pv = cadd(cadd(czero<C>(), cmul(l.one, l.r)), cmul(l.beta, l.pc));
+        const C qcv = cadd(cadd(czero<C>(), cmul(l.one, l.Ap)), cmul(l.beta, l.rc));
+        const C qv = cadd(cadd(cadd(czero<C>(), cmul(l.t0, l.q)), cmul(l.beta, l.rc)), cmul(l.one, qcv));
+        p[o] = pv;
+        qc[o] = qcv;
+        q[o] = qv;
+        return qv;
+    }
+    __device__ __forceinline__ C operator()(int s, long long idx, bool) const { return apply(s, idx, load(s, idx)); }
+};
+
+// CORS: the four vector updates after alpha (CG_Iteration.h:964-1012) in one
+// pass, each output as its separate pass computes it, with r^H r of the new r:
+//   pc = p - alpha q;  rc = qc - alpha Aq;  x += 2 alpha p - alpha^2 q;
+//   r += -2 alpha qc + alpha^2 Aq
+template <typename C>
+__global__ void __launch_bounds__(256) k_cors_update(C* __restrict__ pc, C* __restrict__ rc, C* __restrict__ x,
+                                                     C* __restrict__ r, const C* __restrict__ p,
+                                                     const C* __restrict__ q, const C* __restrict__ qc,
+                                                     const C* __restrict__ Aq, long long n,
+                                                     const double2* __restrict__ S, double2* __restrict__ partial,
+                                                     Gate gate) {
+    if (gate_closed(gate)) return;
+    const C one = coef_c<C>(eval_coef(CoefSpec{-1, 1.0, 0.0}, S));
+    const C mal = coef_c<C>(eval_coef(CoefSpec{S_ALPHA, -1.0, 0.0}, S));
+    const C al2 = coef_c<C>(eval_coef(CoefSpec{S_ALPHA, 2.0, 0.0}, S));
+    const C mt1 = coef_c<C>(eval_coef(CoefSpec{S_T1, -1.0, 0.0}, S));
+    const C mal2 = coef_c<C>(eval_coef(CoefSpec{S_ALPHA, -2.0, 0.0}, S));
+    const C t1 = coef_c<C>(eval_coef(CoefSpec{S_T1, 1.0, 0.0}, S));
+    double2 acc[1] = {make_double2(0, 0)};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const C pi = p[i], qi = q[i], qci = qc[i], aqi = Aq[i];
+        pc[i] = cadd(cadd(czero<C>(), cmul(one, pi)), cmul(mal, qi));
+        rc[i] = cadd(cadd(czero<C>(), cmul(one, qci)), cmul(mal, aqi));
+        x[i] = cadd(cadd(x[i], cmul(al2, pi)), cmul(mt1, qi));
+        const C rv = cadd(cadd(r[i], cmul(mal2, qci)), cmul(t1, aqi));
+        r[i] = rv;
+        acc_dotc(acc[0], rv, rv);
+    }
+    block_reduce_store<1>(acc, partial, blockIdx.x);
+}
+
 // x += alpha p + omega s; r = s - omega t; acc r^H r, b^H r
 template <typename C>
 __global__ void __launch_bounds__(256) k_bicgstab_update(C* __restrict__ x, const C* __restrict__ p,
