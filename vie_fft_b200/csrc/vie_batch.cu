@@ -265,29 +265,6 @@ __global__ void kb_cond(KCtl* const* __restrict__ ctls, int n, cudaGraphConditio
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
-int sms_of_device() {
-    int dev = 0, n = 0;
-    cudaGetDevice(&dev);
-    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n < 1) n = 1;
-    return n;
-}
-// blocks of a persistent kernel: as many as fit on every SM at once
-template <typename K> int persistent_grid(K kernel, int threads, size_t smem) {
-    static std::mutex mu;
-    static std::map<std::tuple<const void*, int, int, size_t>, int> cache;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    const auto key = std::make_tuple(reinterpret_cast<const void*>(kernel), dev, threads, smem);
-    std::lock_guard<std::mutex> lk(mu);
-    auto it = cache.find(key);
-    if (it == cache.end()) {
-        int nb = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, threads, smem) != cudaSuccess || nb < 1) nb = 1;
-        it = cache.emplace(key, nb * sms_of_device()).first;
-    }
-    return it->second;
-}
-
 // the passes of one operator application for the listed instances of a class,
 // each with the block shape and shared memory of the single solve's kernel
 template <typename C, int N, class Pro, class Epi>

@@ -652,6 +652,10 @@ static int solve_cors(vie_ctx* ctx, Operator<T>& op, const cplx_t<T>* b, cplx_t<
     KCtl* ctl = ctx->d_ctl;
     double2* hist = ctx->d_hist;
     const long long nblk = epilogue_blocks(op);
+    // the update kernel in one wave of resident blocks: k_cors_update<float2>
+    // holds 6 blocks per SM, and a grid of kVecBlocks (8 per SM) would leave a
+    // second wave a third full (256^3: 0.79 ms against 0.65 ms in one wave)
+    const int ncu = std::min<int>(kVecBlocks, persistent_grid(k_cors_update<C>, 256, 0));
     auto body = [=, &op]() -> int {
         int rc2;
         ctx->gate = Gate{&ctl->state, KS_RUN};
@@ -667,11 +671,11 @@ static int solve_cors(vie_ctx* ctx, Operator<T>& op, const cplx_t<T>* b, cplx_t<
         if ((rc2 = finalize<1>(ctx, nblk, FinCorsAlpha{}))) return rc2;
         // pc = p - alpha q; rc = qc - alpha Aq (:964-981); x += 2 alpha p - alpha^2 q
         // (:983-997); r += -2 alpha qc + alpha^2 Aq (:999-1012); r^H r: one pass
-        k_cors_update<C><<<kVecBlocks, 256, 0, ctx->stream>>>(pc, rc_, x, r, p, q, qc, Aq, n, ctx->d_scal,
-                                                               ctx->d_partial, ctx->gate);
+        k_cors_update<C><<<ncu, 256, 0, ctx->stream>>>(pc, rc_, x, r, p, q, qc, Aq, n, ctx->d_scal, ctx->d_partial,
+                                                        ctx->gate);
         count_launch();
         VIE_CUDA_TRY(cudaGetLastError(), ctx->err);
-        return finalize<1>(ctx, kVecBlocks, then(FinErr{}, DecideErr{ctl, hist}));
+        return finalize<1>(ctx, ncu, then(FinErr{}, DecideErr{ctl, hist}));
     };
     auto fin = [ctx, &res, verbose]() { return finish(ctx, res, 0, 2, PS_ERR_STEPS, verbose, "CORS"); };
     return launch_or_plan(ctx, plan, body, fin);
