@@ -110,9 +110,17 @@ static int finalize(vie_ctx* ctx, long long nblk, Fin fin) {
     return VIE_OK;
 }
 
+// blocks of a k_lin launch (and reduction partials it writes): one wave of
+// resident blocks, at most kVecBlocks.  Instances with 40 registers hold 6
+// blocks per SM; with kVecBlocks they would run a second wave a third full.
+template <typename C, int NT, int K> static long long lin_blocks() {
+    return std::min<int>(kVecBlocks, persistent_grid(k_lin<C, NT, K>, 256, 0));
+}
+
 template <typename C, int NT, int K>
 static int lin(vie_ctx* ctx, const LinArgs<C, NT, K>& g) {
-    k_lin<C, NT, K><<<kVecBlocks, 256, 0, ctx->stream>>>(g, 3 * ctx->a, ctx->d_scal, ctx->d_partial, ctx->gate);
+    k_lin<C, NT, K><<<(int)lin_blocks<C, NT, K>(), 256, 0, ctx->stream>>>(g, 3 * ctx->a, ctx->d_scal, ctx->d_partial,
+                                                                         ctx->gate);
     count_launch();
     VIE_CUDA_TRY(cudaGetLastError(), ctx->err);
     return VIE_OK;
@@ -725,12 +733,12 @@ static int solve_bicorstab(vie_ctx* ctx, Operator<T>& op, const cplx_t<T>* b, cp
         if ((rc2 = lin(ctx, LinArgs<C, 2, 2>{qc, 0, {{Ap, cs(-1)}, {Aq, cs(S_ALPHA, -1.0)}}, {{pc, 1}, {nullptr, 1}}})))
             return rc2;
         // d0 = conj(pc).qc, so qc^H pc = conj(d0)
-        if ((rc2 = finalize<2>(ctx, kVecBlocks, FinBicorOmega{}))) return rc2;
+        if ((rc2 = finalize<2>(ctx, lin_blocks<C, 2, 2>(), FinBicorOmega{}))) return rc2;
         // x += alpha p + omega pc; r = pc - omega qc; r^H r  (:1289-1315)
         if ((rc2 = lin(ctx, LinArgs<C, 2, 0>{x, 1, {{p, cs(S_ALPHA)}, {pc, cs(S_OMEGA)}}, {}}))) return rc2;
         if ((rc2 = lin(ctx, LinArgs<C, 2, 1>{r, 0, {{pc, cs(-1)}, {qc, cs(S_OMEGA, -1.0)}}, {{nullptr, 1}}})))
             return rc2;
-        return finalize<1>(ctx, kVecBlocks, then(FinErr{}, DecideErr{ctl, hist}));
+        return finalize<1>(ctx, lin_blocks<C, 2, 1>(), then(FinErr{}, DecideErr{ctl, hist}));
     };
     auto fin = [ctx, &res, verbose]() { return finish(ctx, res, 0, 2, PS_STEPS_ONLY, verbose, "BiCORSTAB"); };
     return launch_or_plan(ctx, plan, body, fin);
@@ -769,7 +777,7 @@ static int solve_cg(vie_ctx* ctx, Operator<T>& op, const cplx_t<T>* b, cplx_t<T>
         // x += alpha p; r += alpha Ap; v4 = ||r||^2 (:273-286)
         if ((rc2 = lin(ctx, LinArgs<C, 1, 0>{x, 1, {{p, cs(S_ALPHA)}}, {}}))) return rc2;
         if ((rc2 = lin(ctx, LinArgs<C, 1, 1>{r, 1, {{Ap, cs(S_ALPHA)}}, {{nullptr, 1}}}))) return rc2;
-        if ((rc2 = finalize<1>(ctx, kVecBlocks, FinCgErr{}))) return rc2;
+        if ((rc2 = finalize<1>(ctx, lin_blocks<C, 1, 1>(), FinCgErr{}))) return rc2;
         // q = A^H r; v3 = ||q||^2; beta = v3 / v1 (:291-309)
         if ((rc2 = opmv(ctx, op, ProCopy<C>{r, a}, EpiNorm<C>{q, a}, r, true))) return rc2;
         if ((rc2 = finalize<1>(ctx, nblk, FinCgBeta{}))) return rc2;
@@ -813,7 +821,7 @@ static int solve_bicg(vie_ctx* ctx, Operator<T>& op, const cplx_t<T>* b, cplx_t<
         // x += alpha p; r -= alpha Ap; v2 = r^T r (:463-479)
         if ((rc2 = lin(ctx, LinArgs<C, 1, 0>{x, 1, {{p, cs(S_ALPHA)}}, {}}))) return rc2;
         if ((rc2 = lin(ctx, LinArgs<C, 1, 1>{r, 1, {{Ap, cs(S_ALPHA, -1.0)}}, {{nullptr, 0}}}))) return rc2;
-        if ((rc2 = finalize<1>(ctx, kVecBlocks, FinBicgBeta{}))) return rc2;
+        if ((rc2 = finalize<1>(ctx, lin_blocks<C, 1, 1>(), FinBicgBeta{}))) return rc2;
         // p += beta r (:489-491); then the stop rule (:497-505)
         if ((rc2 = lin(ctx, LinArgs<C, 1, 0>{p, 1, {{r, cs(S_BETA)}}, {}}))) return rc2;
         return finalize<1>(ctx, 1, then(FinNone{}, DecideErr{ctl, hist}));
