@@ -138,7 +138,8 @@ typedef struct {
     int max_iter;       /* iteration cap; <= 0 means nx*ny*nz like the reference */
     double inner_tol;   /* mixed: residual reduction per FP64 refinement step
                            (<= 0: 0.03 for BiCGSTAB's reliable updates, 5e-5 for the
-                           restarted inner solves of the other drivers) */
+                           restarted inner solves of the other drivers, whose last
+                           one stops at 0.9 of the reduction still needed) */
     int max_outer;      /* mixed: refinement cap (<= 0: 30) */
     int verbose;        /* print "CG Error" per iteration like the reference */
     int true_residual;  /* FP64 solves: evaluate ||b - A x|| / ||b|| at exit (one more
