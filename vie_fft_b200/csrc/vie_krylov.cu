@@ -1009,11 +1009,10 @@ int solve_driver(vie_ctx* ctx, const vie_solve_params* prm, vie_solve_info* info
     } else if (prm->precision == VIE_PREC_MIXED) {
         // FP32 inner Krylov inside FP64 defect correction:
         //   r = b - A x (FP64);  solve A d = r / ||r|| in FP32;  x += ||r|| d (FP64)
-        // Default inner reduction 5e-5: two refinement steps reach 1e-8 with a
-        // margin for the gap between the FP32 recursive and the FP64 true
-        // residual.  Measured on the 256^3 solar cell with CORS to 1e-8: 1e-4 ->
-        // 3 steps, 303 FP32 iterations, 2.57 s; 5e-5 -> 2 steps, 292, 2.47 s;
-        // 2e-5 -> 2.49 s; 1e-5 -> 2.66 s.
+        // Default inner reduction 5e-5: two refinement steps reach 1e-8.
+        // Measured on the 256^3 solar cell with CORS to 1e-8: 2e-4 -> 3 steps,
+        // 285 FP32 iterations, 2.30 s; 1e-4 -> 3 steps, 293, 2.37 s; 5e-5, 3e-5
+        // and 2e-5 -> 2 steps, 282, 2.27 s.
         const double inner_tol = prm->inner_tol > 0 ? prm->inner_tol : 5e-5;
         const int max_outer = prm->max_outer > 0 ? prm->max_outer : 30;
         double2* r64 = (double2*)work_vec(ctx, 21, sizeof(double2), &rc);
