@@ -422,7 +422,8 @@ def run_gpu(args, rank, world, local_rank):
         "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "c64 inner + c128 refine", "data": "synthetic",
         "config": workload_config(w, desc, tol_of(args.workload), solver_of(args.workload)),
-        "arm": {"precision": "mixed (FP32 inner Krylov, FP64 reliable updates)",
+        "arm": {"precision": "mixed (FP32 inner Krylov, FP64 "
+                             + ("reliable updates)" if solver_of(args.workload) == "bicgstab" else "defect correction)"),
                 "l2": "inputs larger than L2 (FP32 vectors 403 MB, FP64 805 MB each)",
                 "parallelism": "replicas" if world > 1 else "single"},
         "roofline": {"bound": "hbm", "achieved": ach32, "peak": peak, "unit": "GB/s", "frac": ach32 / peak,
